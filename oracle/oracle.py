@@ -1,0 +1,298 @@
+"""ORACLE — test infrastructure only.
+
+ctypes bindings for
+  * oracle/_ref/libglimpse_ref.so: the reference's own hot-path sources compiled
+    unmodified (oracle/Makefile) behind a C-ABI harness (oracle/ref_harness.cpp);
+  * oracle/_ref/librestate.so: the FP64/FP32 restatement (oracle/restate.c).
+
+Only tests/, __graft_entry__.smoke() and bench.py's reference arm load this
+module; the product path never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.environ.get("GP_ORACLE_LIB", os.path.join(HERE, "_ref", "libglimpse_ref.so"))
+RESTATE_LIB = os.path.join(HERE, "_ref", "librestate.so")
+
+STAGE_INIT, STAGE_BURN, STAGE_MAIN = 0, 1, 2
+
+_ref = None
+_restate = None
+
+
+def _p(a, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype)) if a is not None else None
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        lib = C.CDLL(REF_LIB)
+        vp = C.c_void_p
+        lib.orc_create.restype = vp
+        lib.orc_create.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                   C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint8),
+                                   C.POINTER(C.c_uint8), C.POINTER(C.c_uint8), C.POINTER(C.c_uint8),
+                                   C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
+        lib.orc_destroy.argtypes = [vp]
+        lib.orc_last_error.restype = C.c_char_p
+        lib.orc_last_error.argtypes = [vp]
+        lib.orc_ypacked.restype = C.c_int64
+        lib.orc_ypacked.argtypes = [vp, C.POINTER(C.c_uint8), C.c_int64]
+        lib.orc_asmall.restype = C.c_int64
+        lib.orc_asmall.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.c_int64]
+        lib.orc_asmall_rows.argtypes = [vp]
+        lib.orc_targets.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_uint8), C.POINTER(C.c_uint8)]
+        lib.orc_config.argtypes = [vp, C.c_int, C.c_float, C.c_float, C.c_float, C.c_int, C.c_float, C.c_int,
+                                   C.c_int, C.POINTER(C.c_int), C.c_uint64]
+        lib.orc_iteration.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+        lib.orc_finalize.argtypes = [vp]
+        lib.orc_get_haps.argtypes = [vp, C.c_int, C.POINTER(C.c_uint8), C.POINTER(C.c_uint8)]
+        lib.orc_set_haps.argtypes = [vp, C.c_int, C.POINTER(C.c_uint8), C.POINTER(C.c_uint8)]
+        lib.orc_get_gp.argtypes = [vp, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_uint8),
+                                   C.POINTER(C.c_uint8)]
+        lib.orc_last_states.argtypes = [vp, C.c_int, C.POINTER(C.c_uint32), C.c_int]
+        lib.orc_last_hp.argtypes = [vp, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        lib.orc_pbwt_select.argtypes = [vp, C.c_int, C.c_int]
+        lib.orc_pbwt_levels.argtypes = [vp, C.c_int]
+        lib.orc_pbwt_states.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int32), C.c_int]
+        lib.orc_pbwt_nstored.argtypes = [vp]
+        lib.orc_pbwt_modulo.restype = C.c_float
+        lib.orc_pbwt_modulo.argtypes = [vp]
+        lib.orc_pbwt_groups.argtypes = [vp, C.POINTER(C.c_int32), C.c_int]
+        lib.orc_select.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_uint32), C.c_int]
+        lib.orc_init_select.argtypes = [vp, C.c_int]
+        lib.orc_init_states.argtypes = [vp, C.c_int, C.POINTER(C.c_int32), C.c_int]
+        lib.orc_impute.argtypes = [vp, C.POINTER(C.c_uint32), C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_uint8),
+                                   C.POINTER(C.c_float), C.POINTER(C.c_int32)]
+        lib.orc_rephase.argtypes = [vp, C.POINTER(C.c_uint32), C.c_int, C.POINTER(C.c_uint8), C.POINTER(C.c_uint8),
+                                    C.POINTER(C.c_uint8), C.c_int, C.c_int, C.POINTER(C.c_int32), C.c_int]
+        lib.orc_unphred.argtypes = [C.POINTER(C.c_float)]
+        lib.orc_stream_words.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_int,
+                                         C.POINTER(C.c_uint32)]
+        lib.orc_rng_floats.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.POINTER(C.c_float)]
+        lib.orc_rng_ints.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.POINTER(C.c_uint32),
+                                     C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]
+        lib.orc_std_sample.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int,
+                                       C.POINTER(C.c_int32), C.POINTER(C.c_uint64)]
+        _ref = lib
+    return _ref
+
+
+class RefOracle:
+    """The reference's GLIMPSE2_phase hot path on the host (one object per panel)."""
+
+    def __init__(self, panel, targets=None, *, ne=100000, err_imp=1e-12, err_phase=1e-4, min_gl=1e-10,
+                 pbwt_depth=12, pbwt_modulo_cm=0.1, kinit=1000, kpbwt=2000, kpbwt_target=None, seed=15052011):
+        lib = ref_lib()
+        self.lib = lib
+        self.panel = panel
+        p = panel
+        self._keep = [np.ascontiguousarray(x) for x in (p.bp.astype(np.int32), p.cm.astype(np.float64),
+                                                        p.cref.astype(np.uint32), p.calt.astype(np.uint32),
+                                                        p.lq.astype(np.uint8), p.flag_common.astype(np.uint8),
+                                                        p.major.astype(np.uint8), p.hvar.astype(np.uint8),
+                                                        p.shap_off.astype(np.int64), p.shap_sites.astype(np.int32))]
+        k = self._keep
+        self.h = lib.orc_create(p.n_ref_haps, p.n_sites, _p(k[0], C.c_int), _p(k[1], C.c_double),
+                                _p(k[2], C.c_uint32), _p(k[3], C.c_uint32), _p(k[4], C.c_uint8), _p(k[5], C.c_uint8),
+                                _p(k[6], C.c_uint8), _p(k[7], C.c_uint8), _p(k[8], C.c_int64), _p(k[9], C.c_int32))
+        if not self.h:
+            raise RuntimeError("orc_create failed")
+        self.L = p.n_sites
+        self.seed = seed
+        self.n_targets = 0
+        if targets is not None:
+            self.set_targets(targets)
+            self.configure(ne=ne, err_imp=err_imp, err_phase=err_phase, min_gl=min_gl, pbwt_depth=pbwt_depth,
+                           pbwt_modulo_cm=pbwt_modulo_cm, kinit=kinit, kpbwt=kpbwt, kpbwt_target=kpbwt_target,
+                           seed=seed)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.orc_destroy(self.h)
+            self.h = None
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError(self.lib.orc_last_error(self.h).decode())
+
+    def ypacked(self) -> np.ndarray:
+        n = self.lib.orc_ypacked(self.h, None, 0)
+        out = np.zeros(n, dtype=np.uint8)
+        self.lib.orc_ypacked(self.h, _p(out, C.c_uint8), n)
+        return out
+
+    def a_small_idx(self):
+        rows = self.lib.orc_asmall_rows(self.h)
+        off = np.zeros(rows + 1, dtype=np.int64)
+        tot = self.lib.orc_asmall(self.h, _p(off, C.c_int64), None, 0)
+        vals = np.zeros(max(tot, 1), dtype=np.int32)
+        self.lib.orc_asmall(self.h, _p(off, C.c_int64), _p(vals, C.c_int32), tot)
+        return off, vals[:tot]
+
+    def set_targets(self, targets):
+        self.targets = targets
+        self.n_targets = targets.n
+        self._tk = [np.ascontiguousarray(targets.ploidy.astype(np.int32)),
+                    np.ascontiguousarray(targets.gl.astype(np.uint8)),
+                    np.ascontiguousarray(targets.flat.astype(np.uint8))]
+        self._check(self.lib.orc_targets(self.h, targets.n, _p(self._tk[0], C.c_int), _p(self._tk[1], C.c_uint8),
+                                         _p(self._tk[2], C.c_uint8)))
+
+    def configure(self, *, ne=100000, err_imp=1e-12, err_phase=1e-4, min_gl=1e-10, pbwt_depth=12,
+                  pbwt_modulo_cm=0.1, kinit=1000, kpbwt=2000, kpbwt_target=None, seed=15052011):
+        self.seed = seed
+        kt = None
+        if kpbwt_target is not None:
+            kt = np.ascontiguousarray(np.asarray(kpbwt_target, dtype=np.int32))
+            self._kt = kt
+        self._check(self.lib.orc_config(self.h, ne, err_imp, err_phase, min_gl, pbwt_depth, pbwt_modulo_cm, kinit,
+                                        kpbwt, _p(kt, C.c_int), seed))
+
+    def iteration(self, stage, iter_index, threads=1):
+        self._check(self.lib.orc_iteration(self.h, stage, iter_index, threads))
+
+    def run(self, burnin=5, main=15, threads=1):
+        it = 0
+        self.iteration(STAGE_INIT, it, threads)
+        it += 1
+        for _ in range(burnin):
+            self.iteration(STAGE_BURN, it, threads)
+            it += 1
+        for _ in range(main):
+            self.iteration(STAGE_MAIN, it, threads)
+            it += 1
+        self._check(self.lib.orc_finalize(self.h))
+
+    def haps(self, ind):
+        h0 = np.zeros(self.L, dtype=np.uint8)
+        h1 = np.zeros(self.L, dtype=np.uint8)
+        self.lib.orc_get_haps(self.h, ind, _p(h0, C.c_uint8), _p(h1, C.c_uint8))
+        return h0, h1
+
+    def set_haps(self, ind, h0, h1):
+        h0 = np.ascontiguousarray(h0, dtype=np.uint8)
+        h1 = np.ascontiguousarray(h1, dtype=np.uint8)
+        self.lib.orc_set_haps(self.h, ind, _p(h0, C.c_uint8), _p(h1, C.c_uint8))
+
+    def gp(self, ind):
+        L = self.L
+        gp0 = np.zeros(L, np.float32)
+        gp1 = np.zeros(L, np.float32)
+        hds = np.zeros(L, np.uint8)
+        st = np.zeros(L, np.uint8)
+        cnt = self.lib.orc_get_gp(self.h, ind, _p(gp0, C.c_float), _p(gp1, C.c_float), _p(hds, C.c_uint8),
+                                  _p(st, C.c_uint8))
+        return gp0, gp1, hds, st, cnt
+
+    def last_states(self, ind):
+        out = np.zeros(self.panel.n_ref_haps, np.uint32)
+        n = self.lib.orc_last_states(self.h, ind, _p(out, C.c_uint32), out.size)
+        return out[:n].copy()
+
+    def last_hp(self, ind):
+        hp0 = np.zeros(2 * self.L, np.float32)
+        hp1 = np.zeros(2 * self.L, np.float32)
+        npoly = self.lib.orc_last_hp(self.h, ind, _p(hp0, C.c_float), _p(hp1, C.c_float))
+        return hp0, hp1, npoly
+
+    def pbwt_select(self, iter_index, main_iteration=False):
+        self._check(self.lib.orc_pbwt_select(self.h, iter_index, int(main_iteration)))
+
+    def pbwt_states(self, ind):
+        lv = self.lib.orc_pbwt_levels(self.h, ind)
+        out = []
+        buf = np.zeros(1 << 20, np.int32)
+        for i in range(lv):
+            n = self.lib.orc_pbwt_states(self.h, ind, i, _p(buf, C.c_int32), buf.size)
+            out.append(buf[:n].copy())
+        return out
+
+    def pbwt_groups(self):
+        buf = np.zeros(1 << 20, np.int32)
+        n = self.lib.orc_pbwt_groups(self.h, _p(buf, C.c_int32), buf.size)
+        return buf[:n].copy(), float(self.lib.orc_pbwt_modulo(self.h))
+
+    def select(self, ind, stage):
+        out = np.zeros(self.panel.n_ref_haps, np.uint32)
+        n = self.lib.orc_select(self.h, ind, stage, _p(out, C.c_uint32), out.size)
+        if n < 0:
+            raise RuntimeError(self.lib.orc_last_error(self.h).decode())
+        return out[:n].copy()
+
+    def init_select(self, iter_index=0):
+        self._check(self.lib.orc_init_select(self.h, iter_index))
+
+    def init_states(self, ind):
+        out = np.zeros(self.panel.n_ref_haps, np.int32)
+        n = self.lib.orc_init_states(self.h, ind, _p(out, C.c_int32), out.size)
+        return out[:n].copy()
+
+    def impute(self, states, HL, flat):
+        states = np.ascontiguousarray(states, dtype=np.uint32)
+        HL = np.ascontiguousarray(HL, dtype=np.float32)
+        flat = np.ascontiguousarray(flat, dtype=np.uint8)
+        HP = np.zeros(2 * self.L, np.float32)
+        poly = np.zeros(self.L, np.int32)
+        n = self.lib.orc_impute(self.h, _p(states, C.c_uint32), states.size, _p(HL, C.c_float), _p(flat, C.c_uint8),
+                                _p(HP, C.c_float), _p(poly, C.c_int32))
+        if n < 0:
+            raise RuntimeError(self.lib.orc_last_error(self.h).decode())
+        return HP, poly[:n].copy()
+
+    def rephase(self, states, H0, H1, flat, iter_index, target):
+        states = np.ascontiguousarray(states, dtype=np.uint32)
+        H0 = np.array(H0, dtype=np.uint8, copy=True)
+        H1 = np.array(H1, dtype=np.uint8, copy=True)
+        flat = np.ascontiguousarray(flat, dtype=np.uint8)
+        dip = np.zeros(1 << 20, np.int32)
+        n = self.lib.orc_rephase(self.h, _p(states, C.c_uint32), states.size, _p(H0, C.c_uint8), _p(H1, C.c_uint8),
+                                 _p(flat, C.c_uint8), iter_index, target, _p(dip, C.c_int32), dip.size)
+        if n < 0:
+            raise RuntimeError(self.lib.orc_last_error(self.h).decode())
+        return H0, H1, dip[:n].copy()
+
+
+def unphred_table() -> np.ndarray:
+    out = np.zeros(256, np.float32)
+    ref_lib().orc_unphred(_p(out, C.c_float))
+    return out
+
+
+def stream_words(seed, purpose, iteration, target, start, n):
+    out = np.zeros(n, np.uint32)
+    ref_lib().orc_stream_words(seed, purpose, iteration, target, start, n, _p(out, C.c_uint32))
+    return out
+
+
+def rng_floats(seed, purpose, iteration, target, n):
+    out = np.zeros(n, np.float32)
+    ref_lib().orc_rng_floats(seed, purpose, iteration, target, n, _p(out, C.c_float))
+    return out
+
+
+def rng_ints(seed, purpose, iteration, target, lo, hi):
+    lo = np.ascontiguousarray(lo, np.uint32)
+    hi = np.ascontiguousarray(hi, np.uint32)
+    out = np.zeros(lo.size, np.uint32)
+    used = C.c_uint64(0)
+    ref_lib().orc_rng_ints(seed, purpose, iteration, target, lo.size, _p(lo, C.c_uint32), _p(hi, C.c_uint32),
+                           _p(out, C.c_uint32), C.byref(used))
+    return out, used.value
+
+
+def std_sample(seed, purpose, iteration, target, pop, n):
+    out = np.zeros(max(n, 1), np.int32)
+    used = C.c_uint64(0)
+    k = ref_lib().orc_std_sample(seed, purpose, iteration, target, pop, n, _p(out, C.c_int32), C.byref(used))
+    return out[:k].copy(), used.value

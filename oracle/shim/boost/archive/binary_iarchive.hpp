@@ -1,0 +1,2 @@
+/* Oracle shim: archives are not used on the hot path. */
+#pragma once

@@ -1,0 +1,3 @@
+/* Oracle shim: see serialization.hpp. */
+#pragma once
+#include <boost/serialization/serialization.hpp>
