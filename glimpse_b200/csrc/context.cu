@@ -1,0 +1,286 @@
+// Context creation, panel upload and the call-level C-ABI entry points.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+
+#include "context.h"
+
+namespace gp {
+
+namespace {
+
+// HvarRef (row = common site, MSB-first bytes, bitmatrix.h:89-119) to
+// haplotype-major 32-bit words: refT[h][w] bit i = allele of h at common row 32w+i.
+__global__ void k_transpose_panel(const uint8_t* __restrict__ hvar, int n_com, int stride, int N, int W,
+                                  uint32_t* __restrict__ refT) {
+  const int h = blockIdx.x * blockDim.x + threadIdx.x;
+  const int wi = blockIdx.y;
+  if (h >= N) return;
+  uint32_t word = 0;
+  const int r0 = wi * 32;
+  const int n = min(32, n_com - r0);
+  for (int i = 0; i < n; ++i) {
+    const uint8_t byte = hvar[(size_t)(r0 + i) * stride + (h >> 3)];
+    word |= (uint32_t)((byte >> (7 - (h & 7))) & 1) << i;
+  }
+  refT[(size_t)h * W + wi] = word;
+}
+
+}  // namespace
+
+ModelConst model_constants(const gp_config& c, int n_ref_haps) {
+  ModelConst m;
+  const float err_imp = std::clamp(c.err_imp, 1e-12f, 1e-3f);  // caller_initialise.cpp:152
+  m.ed_imp = err_imp;
+  m.ee_imp = (float)(1.0 - (double)err_imp);                   // conditioning_set.cpp:33-34
+  m.ed_phs = c.err_phase;
+  m.ee_phs = (float)(1.0 - (double)c.err_phase);
+  m.min_gl = c.min_gl;
+  m.nrho = (-0.04 * (double)c.ne) / (double)n_ref_haps;       // conditioning_set.cpp:30
+  m.one_l = 1.0 - 1e-7;
+  return m;
+}
+
+Status Context::fail(int code, const std::string& msg) {
+  err = msg;
+  Status s;
+  s.code = code;
+  s.msg = msg;
+  return s;
+}
+
+int Context::cuda_fail(cudaError_t e, const char* where) {
+  err = std::string(where) + ": " + cudaGetErrorString(e);
+  return GP_E_CUDA;
+}
+
+template <class T>
+static cudaError_t upload(T** dst, const T* src, size_t n, std::vector<void*>& owned) {
+  *dst = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)dst, n * sizeof(T));
+  if (e != cudaSuccess) return e;
+  owned.push_back(*dst);
+  if (src) e = cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
+  return e;
+}
+
+int Context::create_panel(const gp_panel_desc& d) {
+  const int N = d.n_ref_haps, L = d.n_sites;
+  if (N <= 0 || L <= 0 || !d.cm || !d.cref || !d.calt || !d.lq || !d.flag_common || !d.major || !d.shap_off)
+    return (fail(GP_E_ARG, "panel: missing array or empty panel"), GP_E_ARG);
+  host.N = N;
+  host.L = L;
+  host.cm.assign(d.cm, d.cm + L);
+  host.cref.assign(d.cref, d.cref + L);
+  host.calt.assign(d.calt, d.calt + L);
+  host.lq.assign(d.lq, d.lq + L);
+  host.common.assign(d.flag_common, d.flag_common + L);
+  host.major.assign(d.major, d.major + L);
+  host.comrow.assign(L, -1);
+  int nc = 0, nchq = 0;
+  for (int l = 0; l < L; ++l)
+    if (host.common[l]) {
+      host.comrow[l] = nc++;
+      if (!host.lq[l]) ++nchq;
+    }
+  host.n_com = nc;
+  host.n_com_hq = nchq;
+  const int stride = (N + 7) / 8;
+  if (nc > 0 && !d.hvar) return (fail(GP_E_ARG, "panel: hvar missing"), GP_E_ARG);
+  host.hvar.assign(d.hvar, d.hvar + (size_t)nc * stride);
+  const int64_t nnz = d.shap_off[N];
+  host.shap_off.assign(d.shap_off, d.shap_off + N + 1);
+  host.shap_sites.assign(d.shap_sites, d.shap_sites + nnz);
+  for (int64_t j = 0; j < nnz; ++j)
+    if (host.shap_sites[j] < 0 || host.shap_sites[j] >= L || host.common[host.shap_sites[j]])
+      return (fail(GP_E_DATA, "panel: ShapRef lists a site that is not a rare site"), GP_E_DATA);
+
+  DevPanel& P = panel;
+  P.N = N;
+  P.L = L;
+  P.n_com = nc;
+  P.n_com_hq = nchq;
+  P.W = std::max(1, (nc + 31) / 32);
+  P.shap_nnz = nnz;
+  cudaError_t e;
+  if ((e = upload(&P.cm, host.cm.data(), L, owned)) != cudaSuccess) return cuda_fail(e, "panel cm");
+  if ((e = upload(&P.lq, host.lq.data(), L, owned)) != cudaSuccess) return cuda_fail(e, "panel lq");
+  if ((e = upload(&P.common, host.common.data(), L, owned)) != cudaSuccess) return cuda_fail(e, "panel common");
+  if ((e = upload(&P.major, host.major.data(), L, owned)) != cudaSuccess) return cuda_fail(e, "panel major");
+  if ((e = upload(&P.cref, host.cref.data(), L, owned)) != cudaSuccess) return cuda_fail(e, "panel cref");
+  if ((e = upload(&P.calt, host.calt.data(), L, owned)) != cudaSuccess) return cuda_fail(e, "panel calt");
+  if ((e = upload(&P.comrow, host.comrow.data(), L, owned)) != cudaSuccess) return cuda_fail(e, "panel comrow");
+  if ((e = upload(&P.shap_off, host.shap_off.data(), N + 1, owned)) != cudaSuccess) return cuda_fail(e, "shap_off");
+  if ((e = upload(&P.shap_sites, host.shap_sites.data(), (size_t)nnz, owned)) != cudaSuccess)
+    return cuda_fail(e, "shap_sites");
+  if ((e = upload(&P.refT, (const uint32_t*)nullptr, (size_t)N * P.W, owned)) != cudaSuccess)
+    return cuda_fail(e, "refT");
+  if (nc > 0) {
+    uint8_t* dh = nullptr;
+    if ((e = cudaMalloc(&dh, host.hvar.size())) != cudaSuccess) return cuda_fail(e, "hvar staging");
+    e = cudaMemcpy(dh, host.hvar.data(), host.hvar.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+      dim3 g((N + 255) / 256, P.W);
+      k_transpose_panel<<<g, 256, 0, stream>>>(dh, nc, stride, N, P.W, P.refT);
+      e = cudaStreamSynchronize(stream);
+    }
+    cudaFree(dh);
+    if (e != cudaSuccess) return cuda_fail(e, "panel transpose");
+  } else {
+    cudaMemsetAsync(P.refT, 0, sizeof(uint32_t) * N * P.W, stream);
+  }
+  return GP_OK;
+}
+
+Context::~Context() {
+  cudaStreamSynchronize(stream);
+  for (void* p : owned) cudaFree(p);
+  impute.states.release(); impute.nstates.release(); impute.states_off.release();
+  impute.mark.release(); impute.polyidx.release(); impute.poly.release(); impute.npoly.release();
+  impute.hvar.release(); impute.em.release(); impute.tr.release(); impute.fl.release();
+  impute.alpha.release(); impute.alpha_off.release();
+  impute.hl.release(); impute.hp.release(); impute.flat.release();
+  if (stream) cudaStreamDestroy(stream);
+}
+
+// Conditioning sets from explicit state lists, then the forward-backward.
+// hl/flat/hp are device pointers laid out n x 2L / n x L / n x 2L.
+int Context::impute_device(int n, const std::vector<int64_t>& off, const std::vector<uint32_t>& states,
+                           const float* d_hl, const uint8_t* d_flat, float* d_hp) {
+  const int L = panel.L;
+  int Kmax = 0;
+  for (int i = 0; i < n; ++i) Kmax = std::max<int>(Kmax, (int)(off[i + 1] - off[i]));
+  if (Kmax <= 0) return (fail(GP_E_DATA, "conditioning set is empty"), GP_E_DATA);
+  if (Kmax > kMaxStates)
+    return (fail(GP_E_ARG, "conditioning set larger than " + std::to_string(kMaxStates) + " states"), GP_E_ARG);
+  ImputeWork& w = impute;
+  w.n = n;
+  w.L = L;
+  w.Kp = (Kmax + 31) / 32 * 32;
+  w.WB = (L + 31) / 32;
+  // states padded to Kp per entry
+  std::vector<uint32_t> hs((size_t)n * w.Kp, 0u);
+  std::vector<int32_t> hn(n);
+  for (int i = 0; i < n; ++i) {
+    hn[i] = (int32_t)(off[i + 1] - off[i]);
+    for (int64_t j = off[i]; j < off[i + 1]; ++j) {
+      const uint32_t h = states[j];
+      if ((int)h >= panel.N) return (fail(GP_E_ARG, "state id out of range"), GP_E_ARG);
+      if (j > off[i] && states[j - 1] >= h)
+        return (fail(GP_E_ARG, "state ids must be sorted and unique"), GP_E_ARG);
+      hs[(size_t)i * w.Kp + (j - off[i])] = h;
+    }
+  }
+  cudaError_t e;
+  if ((e = w.states.ensure(hs.size() * 4)) != cudaSuccess) return cuda_fail(e, "alloc states");
+  if ((e = w.nstates.ensure(n * 4)) != cudaSuccess) return cuda_fail(e, "alloc nstates");
+  if ((e = w.mark.ensure((size_t)n * L)) != cudaSuccess) return cuda_fail(e, "alloc mark");
+  if ((e = w.polyidx.ensure((size_t)n * L * 4)) != cudaSuccess) return cuda_fail(e, "alloc polyidx");
+  if ((e = w.poly.ensure((size_t)n * L * 4)) != cudaSuccess) return cuda_fail(e, "alloc poly");
+  if ((e = w.npoly.ensure(n * 4)) != cudaSuccess) return cuda_fail(e, "alloc npoly");
+  if ((e = w.hvar.ensure((size_t)n * w.WB * w.Kp * 4)) != cudaSuccess) return cuda_fail(e, "alloc hvar");
+  if ((e = w.em.ensure((size_t)n * L * 16)) != cudaSuccess) return cuda_fail(e, "alloc em");
+  if ((e = w.tr.ensure((size_t)n * L * 8)) != cudaSuccess) return cuda_fail(e, "alloc tr");
+  if ((e = w.fl.ensure((size_t)n * L)) != cudaSuccess) return cuda_fail(e, "alloc fl");
+  if ((e = w.alpha_off.ensure((size_t)n * 8)) != cudaSuccess) return cuda_fail(e, "alloc alpha_off");
+  cudaMemcpyAsync(w.states.ptr, hs.data(), hs.size() * 4, cudaMemcpyHostToDevice, stream);
+  cudaMemcpyAsync(w.nstates.ptr, hn.data(), n * 4, cudaMemcpyHostToDevice, stream);
+
+  launch_mark_poly(panel, w, stream);
+  launch_compact_poly(panel, w, stream);
+  launch_build_hvar(panel, w, stream);
+  launch_site_records(panel, mc, w, d_hl, d_flat, stream);
+  std::vector<int32_t> np(n);
+  cudaMemcpyAsync(np.data(), w.npoly.ptr, n * 4, cudaMemcpyDeviceToHost, stream);
+  if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(e, "conditioning set");
+  std::vector<int64_t> aoff(n);
+  int64_t tot = 0;
+  for (int i = 0; i < n; ++i) {
+    aoff[i] = tot;
+    tot += (int64_t)np[i] * w.Kp;
+  }
+  if ((e = w.alpha.ensure((size_t)std::max<int64_t>(tot, 1) * 4)) != cudaSuccess)
+    return cuda_fail(e, "alloc alpha");
+  cudaMemcpyAsync(w.alpha_off.ptr, aoff.data(), n * 8, cudaMemcpyHostToDevice, stream);
+  launch_impute_fb(mc, w, d_hp, stream);
+  launch_impute_mono(panel, mc, w, d_hl, d_flat, d_hp, stream);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "imputation launch");
+  return GP_OK;
+}
+
+}  // namespace gp
+
+using gp::Context;
+
+extern "C" {
+
+void gp_config_defaults(gp_config* c) {
+  if (!c) return;
+  c->ne = 100000;
+  c->err_imp = 1e-12f;
+  c->err_phase = 1e-4f;
+  c->min_gl = 1e-10f;
+  c->pbwt_depth = 12;
+  c->pbwt_modulo_cm = 0.1f;
+  c->kinit = 1000;
+  c->kpbwt = 2000;
+  c->seed = 15052011ull;
+  c->device = 0;
+}
+
+int gp_ctx_create(const gp_panel_desc* panel, const gp_config* cfg, gp_ctx** out) {
+  if (!panel || !cfg || !out) return GP_E_ARG;
+  *out = nullptr;
+  int dev_count = 0;
+  if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count <= cfg->device) return GP_E_CUDA;
+  if (cudaSetDevice(cfg->device) != cudaSuccess) return GP_E_CUDA;
+  std::unique_ptr<Context> c(new (std::nothrow) Context());
+  if (!c) return GP_E_NOMEM;
+  c->cfg = *cfg;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return GP_E_CUDA;
+  int rc = c->create_panel(*panel);
+  if (rc != GP_OK) {
+    std::fprintf(stderr, "gp_ctx_create: %s\n", c->err.c_str());
+    return rc;
+  }
+  c->mc = gp::model_constants(*cfg, panel->n_ref_haps);
+  *out = reinterpret_cast<gp_ctx*>(c.release());
+  return GP_OK;
+}
+
+int gp_ctx_destroy(gp_ctx* ctx) {
+  delete reinterpret_cast<Context*>(ctx);
+  return GP_OK;
+}
+
+const char* gp_last_error(const gp_ctx* ctx) {
+  return ctx ? reinterpret_cast<const Context*>(ctx)->err.c_str() : "null context";
+}
+
+int gp_impute_batch(gp_ctx* ctx, int32_t n, const int64_t* states_off, const uint32_t* states, const float* hl,
+                    const uint8_t* flat, float* hp) {
+  if (!ctx) return GP_E_ARG;
+  Context& c = *reinterpret_cast<Context*>(ctx);
+  if (n <= 0 || !states_off || !states || !hl || !flat || !hp) return (c.fail(GP_E_ARG, "impute: bad argument"), GP_E_ARG);
+  const int L = c.panel.L;
+  std::vector<int64_t> off(states_off, states_off + n + 1);
+  std::vector<uint32_t> st(states, states + off[n]);
+  cudaError_t e;
+  gp::ImputeWork& w = c.impute;
+  if ((e = w.hl.ensure((size_t)n * 2 * L * 4)) != cudaSuccess) return c.cuda_fail(e, "alloc hl");
+  if ((e = w.hp.ensure((size_t)n * 2 * L * 4)) != cudaSuccess) return c.cuda_fail(e, "alloc hp");
+  if ((e = w.flat.ensure((size_t)n * L)) != cudaSuccess) return c.cuda_fail(e, "alloc flat");
+  cudaMemcpyAsync(w.hl.ptr, hl, (size_t)n * 2 * L * 4, cudaMemcpyHostToDevice, c.stream);
+  cudaMemcpyAsync(w.flat.ptr, flat, (size_t)n * L, cudaMemcpyHostToDevice, c.stream);
+  int rc = c.impute_device(n, off, st, w.hl.as<float>(), w.flat.as<uint8_t>(), w.hp.as<float>());
+  if (rc != GP_OK) return rc;
+  cudaMemcpyAsync(hp, w.hp.ptr, (size_t)n * 2 * L * 4, cudaMemcpyDeviceToHost, c.stream);
+  if ((e = cudaStreamSynchronize(c.stream)) != cudaSuccess) return c.cuda_fail(e, "impute");
+  return GP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,90 @@
+// Internal declarations shared by the CUDA translation units of libglimpse_b200.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/glimpse_b200.h"
+#include "replay_rng.h"
+
+namespace gp {
+
+constexpr int kWarp = 32;
+constexpr int kImputeThreads = 256;           // threads per haplotype in the imputation HMM
+constexpr int kImputeStatesPerThread = 8;     // registers per thread for owned states
+constexpr int kMaxStates = kImputeThreads * kImputeStatesPerThread;  // 2048
+constexpr int kHaps = 8;                      // HAP_NUMBER (phasing_hmm.h:38)
+
+// Status carried out of host helpers.
+struct Status {
+  int code = GP_OK;
+  std::string msg;
+};
+
+// Growable device buffer (bytes); contents are not preserved on growth.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    size_t want = bytes + bytes / 8 + 256;
+    cudaError_t e = cudaMalloc(&ptr, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+  }
+  template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Panel resident in device memory.
+struct DevPanel {
+  int N = 0, L = 0, n_com = 0, n_com_hq = 0, W = 0;  // W: 32-bit words per haplotype over common rows
+  double* cm = nullptr;
+  uint8_t* lq = nullptr;
+  uint8_t* common = nullptr;
+  uint8_t* major = nullptr;
+  uint32_t* cref = nullptr;
+  uint32_t* calt = nullptr;
+  int32_t* comrow = nullptr;       // site -> common row, -1 for rare
+  uint32_t* refT = nullptr;        // [N][W] haplotype-major bits over common rows (bit r%32 of word r/32)
+  int64_t* shap_off = nullptr;     // [N+1]
+  int32_t* shap_sites = nullptr;   // rare sites carrying the non-major allele, per haplotype
+  int64_t shap_nnz = 0;
+};
+
+// Per-batch scratch for the imputation path (sized for n haplotypes).
+struct ImputeWork {
+  int n = 0, L = 0, Kp = 0, WB = 0;  // WB: 32-site blocks per haplotype (upper bound)
+  DevBuf states, nstates, states_off;
+  DevBuf mark, polyidx, poly, npoly;
+  DevBuf hvar, em, tr, fl;
+  DevBuf alpha, alpha_off;
+  DevBuf hl, hp, flat;
+};
+
+// Model constants derived from gp_config the way the reference derives them
+// (conditioning_set.cpp:27-37, caller_initialise.cpp:150-153).
+struct ModelConst {
+  float ed_imp, ee_imp, ed_phs, ee_phs, min_gl;
+  double nrho, one_l;
+};
+
+// Kernel launchers (kernels_impute.cu).
+void launch_mark_poly(const DevPanel& P, ImputeWork& w, cudaStream_t s);
+void launch_compact_poly(const DevPanel& P, ImputeWork& w, cudaStream_t s);
+void launch_build_hvar(const DevPanel& P, ImputeWork& w, cudaStream_t s);
+void launch_site_records(const DevPanel& P, const ModelConst& mc, ImputeWork& w, const float* hl,
+                         const uint8_t* flat, cudaStream_t s);
+void launch_impute_fb(const ModelConst& mc, ImputeWork& w, float* hp, cudaStream_t s);
+void launch_impute_mono(const DevPanel& P, const ModelConst& mc, ImputeWork& w, const float* hl,
+                        const uint8_t* flat, float* hp, cudaStream_t s);
+
+}  // namespace gp

@@ -1,0 +1,163 @@
+/*
+ * glimpse_b200 — C-ABI of the B200 implementation of GLIMPSE2_phase's inner
+ * loop: PBWT conditioning-state selection, the haploid Li-Stephens
+ * forward-backward (imputation HMM), the 8-hypothesis phasing HMM with Gibbs
+ * phase resampling, and genotype-posterior / dosage accumulation.
+ *
+ * The reference has no FFI for this path; its seams are C++ methods called by
+ * the Gibbs driver (phase/src/caller/caller_algorithm.cpp:53-126). Each entry
+ * point below names the method(s) it replaces.
+ *
+ * Conventions
+ *  - Every function returns GP_OK (0) or a negative GP_E* status; none exits
+ *    or aborts. gp_last_error(ctx) describes the last failure.
+ *  - Host buffers are owned by the caller and are only read/written during
+ *    the call. Device memory is owned by the context.
+ *  - One host thread per context; all work runs on the context's CUDA stream.
+ *  - Sites are indexed 0..n_sites-1 in panel order; haplotype bits are 0/1.
+ *  - Random numbers come from counter-based streams keyed by
+ *    (seed, purpose, iteration, target); see glimpse_b200/csrc/replay_rng.h.
+ */
+#ifndef GLIMPSE_B200_H
+#define GLIMPSE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GP_OK 0
+#define GP_E_ARG (-1)      /* invalid argument / size */
+#define GP_E_CUDA (-2)     /* CUDA runtime error */
+#define GP_E_NOMEM (-3)    /* device or host allocation failed */
+#define GP_E_STATE (-4)    /* call out of order (e.g. no targets set) */
+#define GP_E_DATA (-5)     /* inconsistent input data (e.g. zero states) */
+
+#define GP_STAGE_INIT 0
+#define GP_STAGE_BURN 1
+#define GP_STAGE_MAIN 2
+
+typedef struct gp_ctx gp_ctx;
+
+/* Reference panel in the reference's in-memory representation
+ * (common/src/containers/ref_haplotype_set.h:60-75, variant.h:33-45). */
+typedef struct gp_panel_desc {
+  int32_t n_ref_haps;          /* N */
+  int32_t n_sites;             /* L */
+  const double* cm;            /* [L] genetic position, cM */
+  const uint32_t* cref;        /* [L] reference allele count in the panel */
+  const uint32_t* calt;        /* [L] alternative allele count in the panel */
+  const uint8_t* lq;           /* [L] low-quality site flag (variant::LQ) */
+  const uint8_t* flag_common;  /* [L] 1 = common (plain bit matrix), 0 = rare (sparse) */
+  const uint8_t* major;        /* [L] major allele (calt > cref) */
+  const uint8_t* hvar;         /* HvarRef: n_common rows x ceil(N/8) bytes, MSB first */
+  const int64_t* shap_off;     /* ShapRef CSR offsets [N+1] */
+  const int32_t* shap_sites;   /* ShapRef CSR values: rare sites carrying the non-major allele */
+  /* Optional sparse PBWT (ref_haplotype_set.h:70-71). NULL: built by gp_ctx_create. */
+  const uint8_t* ypacked;
+  int64_t ypacked_len;
+  const int64_t* asmall_off;   /* [n_common_hq + 2] */
+  const int32_t* asmall_idx;
+} gp_panel_desc;
+
+/* Model and selection parameters (phase/src/caller/caller_parameters.cpp:30-101). */
+typedef struct gp_config {
+  int32_t ne;                  /* --ne, default 100000 */
+  float err_imp;               /* --err-imp, default 1e-12 (clamped to [1e-12, 1e-3]) */
+  float err_phase;             /* --err-phase, default 1e-4 */
+  float min_gl;                /* --min-gl, default 1e-10 */
+  int32_t pbwt_depth;          /* --pbwt-depth, default 12 */
+  float pbwt_modulo_cm;        /* --pbwt-modulo-cm, default 0.1 */
+  int32_t kinit;               /* --Kinit, default 1000 */
+  int32_t kpbwt;               /* --Kpbwt, default 2000 (per-target override in gp_targets_set) */
+  uint64_t seed;               /* --seed, default 15052011 */
+  int32_t device;              /* CUDA device ordinal */
+} gp_config;
+
+/* Fill a config with the reference's defaults. */
+void gp_config_defaults(gp_config* cfg);
+
+/* Upload the panel (replaces reading the binary panel in
+ * caller_initialise.cpp:93-104 and haplotype_set::allocatePBWT,
+ * haplotype_set.cpp:229-315) and create a context. */
+int gp_ctx_create(const gp_panel_desc* panel, const gp_config* cfg, gp_ctx** out);
+int gp_ctx_destroy(gp_ctx* ctx);
+const char* gp_last_error(const gp_ctx* ctx);
+
+/* Targets (genotype_set / genotype objects, genotype.h:81-136).
+ * gl: n x L x 3 phred bytes (ploidy+1 used per site), flat: n x L,
+ * ploidy: n (1 or 2), kpbwt: n per-target Kpbwt or NULL for cfg->kpbwt. */
+int gp_targets_set(gp_ctx* ctx, int32_t n, const uint8_t* gl, const uint8_t* flat, const int32_t* ploidy,
+                   const int32_t* kpbwt);
+
+/* One Gibbs iteration over all targets (caller::phase_iteration,
+ * caller_algorithm.cpp:86-126, with phase_individual :53-84 for every target):
+ * selection, haplotype likelihoods, two imputation passes with sampling,
+ * phasing, and in the main stage the genotype-posterior accumulation.
+ * iteration keys the random streams (0 = init, then 1, 2, ...). */
+int gp_iteration(gp_ctx* ctx, int32_t stage, int32_t iteration);
+
+/* Whole run: 1 init + burnin + main iterations, then finalisation
+ * (caller::phase_loop, caller_algorithm.cpp:223-243). */
+int gp_run(gp_ctx* ctx, int32_t burnin, int32_t main);
+
+/* Current haplotypes (checkpoint/resume stays with the caller,
+ * caller_algorithm.cpp:136-221). h0/h1: n x L bytes. */
+int gp_haps_get(gp_ctx* ctx, uint8_t* h0, uint8_t* h1);
+int gp_haps_set(gp_ctx* ctx, const uint8_t* h0, const uint8_t* h1);
+
+/* Per-site haplotype posteriors of the last iteration for one target
+ * (HP0/HP1 of phase_individual): hp0/hp1: 2 x L floats. */
+int gp_posteriors_get(gp_ctx* ctx, int32_t target, float* hp0, float* hp1);
+
+/* Conditioning states of the last iteration for one target
+ * (conditioning_set::idxHaps_ref, conditioning_set.h:62). Returns the count
+ * through n_out; states must hold at least n_ref_haps entries. */
+int gp_states_get(gp_ctx* ctx, int32_t target, uint32_t* states, int32_t* n_out);
+
+/* Finalised genotype posteriors and dosages (genotype::sortAndNormAndInferGenotype,
+ * genotype.cpp:211-244, and the DS/GP fields of genotype_writer.cpp:98-160):
+ * all arrays n x L. gp0/gp1 as stored (GP of genotypes 0 and 1), ds the dosage
+ * gp1 + 2*gp2 rounded to 1e-3, gt0/gt1 the called alleles (hds-phased hets). */
+int gp_finalize(gp_ctx* ctx);
+int gp_gp_get(gp_ctx* ctx, float* gp0, float* gp1, float* ds, uint8_t* gt0, uint8_t* gt1);
+
+/* ---- Call-level entry points (one reference method, batched) ---- */
+
+/* imputation_hmm::computePosteriors(HL, flat, HP) (imputation_hmm.h:59)
+ * for n independent haplotypes, each with an explicit conditioning set given
+ * as sorted reference-haplotype ids (states_off[n+1], states). hl, hp: n x 2L;
+ * flat: n x L. The conditioning set is built as
+ * conditioning_set::compactSelection builds it (conditioning_set.cpp:123-196). */
+int gp_impute_batch(gp_ctx* ctx, int32_t n, const int64_t* states_off, const uint32_t* states, const float* hl,
+                    const uint8_t* flat, float* hp);
+
+/* phasing_hmm::rephaseHaplotypes(H0, H1, flat) (phasing_hmm.h:136) for n
+ * diploid targets with explicit conditioning sets; h0/h1 updated in place
+ * (n x L). Target t draws from stream (RNG_PHASE, iteration, target_ids[t]). */
+int gp_rephase_batch(gp_ctx* ctx, int32_t n, const int64_t* states_off, const uint32_t* states, uint8_t* h0,
+                     uint8_t* h1, const uint8_t* flat, int32_t iteration, const int32_t* target_ids);
+
+/* haplotype_set::matchHapsFromCompressedPBWTSmall (haplotype_set.cpp:317-394)
+ * from the current target haplotypes, followed by the state union of
+ * conditioning_set::compactSelection (conditioning_set.cpp:96-104). */
+int gp_select(gp_ctx* ctx, int32_t stage, int32_t iteration);
+
+/* pbwt_states of the last selection for one target, level by level
+ * (haplotype_set.h:95): fills counts[pbwt_depth] and states (concatenated). */
+int gp_pbwt_states_get(gp_ctx* ctx, int32_t target, int32_t* counts, int32_t* states, int32_t cap);
+
+/* Sparse PBWT of the panel (ref_haplotype_set::build_sparsePBWT,
+ * ref_haplotype_set.cpp:47-103): returns lengths, copies when buffers are given. */
+int gp_sparse_pbwt_get(gp_ctx* ctx, uint8_t* ypacked, int64_t* ypacked_len, int64_t* asmall_off,
+                       int32_t* asmall_idx, int64_t* asmall_len);
+
+/* Timing of the last gp_iteration by stage, in milliseconds (device events). */
+int gp_stage_times(gp_ctx* ctx, float* ms, int32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GLIMPSE_B200_H */
