@@ -7,6 +7,7 @@
 #include <numeric>
 
 #include "context.h"
+#include "phase.h"
 
 namespace gp {
 
@@ -144,17 +145,18 @@ Context::~Context() {
   impute.hvar.release(); impute.em.release(); impute.tr.release(); impute.fl.release();
   impute.alpha.release(); impute.alpha_off.release();
   impute.hl.release(); impute.hp.release(); impute.flat.release();
+  for (DevBuf* b : phase.all()) b->release();
   if (stream) cudaStreamDestroy(stream);
 }
 
-// Conditioning sets from explicit state lists, then the forward-backward.
-// hl/flat/hp are device pointers laid out n x 2L / n x L / n x 2L.
-int Context::impute_device(int n, const std::vector<int64_t>& off, const std::vector<uint32_t>& states,
-                           const float* d_hl, const uint8_t* d_flat, float* d_hp) {
+// Conditioning sets from explicit state lists (sorted ids per entry): poly
+// sites, Hvar words. Leaves npoly on the host in impute_np.
+int Context::build_condsets(int n, const std::vector<int64_t>& off, const std::vector<uint32_t>& states) {
   const int L = panel.L;
   int Kmax = 0;
   for (int i = 0; i < n; ++i) Kmax = std::max<int>(Kmax, (int)(off[i + 1] - off[i]));
-  if (Kmax <= 0) return (fail(GP_E_DATA, "conditioning set is empty"), GP_E_DATA);
+  for (int i = 0; i < n; ++i)
+    if (off[i + 1] == off[i]) return (fail(GP_E_DATA, "conditioning set is empty"), GP_E_DATA);
   if (Kmax > kMaxStates)
     return (fail(GP_E_ARG, "conditioning set larger than " + std::to_string(kMaxStates) + " states"), GP_E_ARG);
   ImputeWork& w = impute;
@@ -162,7 +164,6 @@ int Context::impute_device(int n, const std::vector<int64_t>& off, const std::ve
   w.L = L;
   w.Kp = (Kmax + 31) / 32 * 32;
   w.WB = (L + 31) / 32;
-  // states padded to Kp per entry
   std::vector<uint32_t> hs((size_t)n * w.Kp, 0u);
   std::vector<int32_t> hn(n);
   for (int i = 0; i < n; ++i) {
@@ -175,6 +176,7 @@ int Context::impute_device(int n, const std::vector<int64_t>& off, const std::ve
       hs[(size_t)i * w.Kp + (j - off[i])] = h;
     }
   }
+  host_nstates = hn;
   cudaError_t e;
   if ((e = w.states.ensure(hs.size() * 4)) != cudaSuccess) return cuda_fail(e, "alloc states");
   if ((e = w.nstates.ensure(n * 4)) != cudaSuccess) return cuda_fail(e, "alloc nstates");
@@ -183,32 +185,112 @@ int Context::impute_device(int n, const std::vector<int64_t>& off, const std::ve
   if ((e = w.poly.ensure((size_t)n * L * 4)) != cudaSuccess) return cuda_fail(e, "alloc poly");
   if ((e = w.npoly.ensure(n * 4)) != cudaSuccess) return cuda_fail(e, "alloc npoly");
   if ((e = w.hvar.ensure((size_t)n * w.WB * w.Kp * 4)) != cudaSuccess) return cuda_fail(e, "alloc hvar");
+  cudaMemcpyAsync(w.states.ptr, hs.data(), hs.size() * 4, cudaMemcpyHostToDevice, stream);
+  cudaMemcpyAsync(w.nstates.ptr, hn.data(), n * 4, cudaMemcpyHostToDevice, stream);
+  launch_mark_poly(panel, w, stream);
+  launch_compact_poly(panel, w, stream);
+  launch_build_hvar(panel, w, stream);
+  impute_np.assign(n, 0);
+  cudaMemcpyAsync(impute_np.data(), w.npoly.ptr, n * 4, cudaMemcpyDeviceToHost, stream);
+  if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(e, "conditioning set");
+  return GP_OK;
+}
+
+// Forward-backward over the current conditioning sets.
+int Context::run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
+  ImputeWork& w = impute;
+  const int n = w.n, L = w.L;
+  cudaError_t e;
   if ((e = w.em.ensure((size_t)n * L * 16)) != cudaSuccess) return cuda_fail(e, "alloc em");
   if ((e = w.tr.ensure((size_t)n * L * 8)) != cudaSuccess) return cuda_fail(e, "alloc tr");
   if ((e = w.fl.ensure((size_t)n * L)) != cudaSuccess) return cuda_fail(e, "alloc fl");
   if ((e = w.alpha_off.ensure((size_t)n * 8)) != cudaSuccess) return cuda_fail(e, "alloc alpha_off");
-  cudaMemcpyAsync(w.states.ptr, hs.data(), hs.size() * 4, cudaMemcpyHostToDevice, stream);
-  cudaMemcpyAsync(w.nstates.ptr, hn.data(), n * 4, cudaMemcpyHostToDevice, stream);
-
-  launch_mark_poly(panel, w, stream);
-  launch_compact_poly(panel, w, stream);
-  launch_build_hvar(panel, w, stream);
-  launch_site_records(panel, mc, w, d_hl, d_flat, stream);
-  std::vector<int32_t> np(n);
-  cudaMemcpyAsync(np.data(), w.npoly.ptr, n * 4, cudaMemcpyDeviceToHost, stream);
-  if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(e, "conditioning set");
   std::vector<int64_t> aoff(n);
   int64_t tot = 0;
   for (int i = 0; i < n; ++i) {
     aoff[i] = tot;
-    tot += (int64_t)np[i] * w.Kp;
+    tot += (int64_t)impute_np[i] * w.Kp;
   }
-  if ((e = w.alpha.ensure((size_t)std::max<int64_t>(tot, 1) * 4)) != cudaSuccess)
-    return cuda_fail(e, "alloc alpha");
+  if ((e = w.alpha.ensure((size_t)std::max<int64_t>(tot, 1) * 4)) != cudaSuccess) return cuda_fail(e, "alloc alpha");
   cudaMemcpyAsync(w.alpha_off.ptr, aoff.data(), n * 8, cudaMemcpyHostToDevice, stream);
+  launch_site_records(panel, mc, w, d_hl, d_flat, stream);
   launch_impute_fb(mc, w, d_hp, stream);
   launch_impute_mono(panel, mc, w, d_hl, d_flat, d_hp, stream);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "imputation launch");
+  return GP_OK;
+}
+
+// Phasing for nb entries of the current conditioning sets (tsel: device list of
+// entry indices or null for 0..nb-1; target_ids: device stream targets or null).
+int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_host, int nb, uint8_t* d_h0,
+                       uint8_t* d_h1, const uint8_t* d_flat, int iteration, const int32_t* d_target_ids) {
+  ImputeWork& w = impute;
+  PhaseWork& p = phase;
+  const int L = panel.L;
+  cudaError_t e;
+  if ((e = p.rel.ensure((size_t)nb * L * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.code.ensure((size_t)nb * L)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.seg.ensure((size_t)nb * L * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.miss.ensure((size_t)nb * L * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.seg_start.ensure((size_t)nb * (L + 2) * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.counts.ensure((size_t)nb * 3 * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  PhaseVars V;
+  V.rel = p.rel.as<int32_t>();
+  V.code = p.code.as<uint8_t>();
+  V.seg = p.seg.as<int32_t>();
+  V.miss = p.miss.as<int32_t>();
+  V.seg_start = p.seg_start.as<int32_t>();
+  V.nvar = p.counts.as<int32_t>();
+  V.nseg = V.nvar + nb;
+  V.nmiss = V.nvar + 2 * nb;
+  launch_build_vars(d_tsel, nb, w.poly.as<int32_t>(), w.npoly.as<int32_t>(), d_h0, d_h1, d_flat, panel.lq, L, V,
+                    stream);
+  std::vector<int32_t> cnt((size_t)nb * 3);
+  cudaMemcpyAsync(cnt.data(), p.counts.ptr, cnt.size() * 4, cudaMemcpyDeviceToHost, stream);
+  if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(e, "phasing vars");
+  std::vector<int64_t> poff(nb), ioff(nb);
+  int64_t ptot = 0, itot = 0;
+  int Kmax = 0;
+  for (int b = 0; b < nb; ++b) {
+    const int t = tsel_host.empty() ? b : tsel_host[b];
+    const int K = host_nstates[t];
+    Kmax = std::max(Kmax, K);
+    poff[b] = ptot;
+    ioff[b] = itot;
+    ptot += (int64_t)cnt[nb + b] * K * 8;
+    itot += (int64_t)cnt[2 * nb + b] * K * 8;
+  }
+  if ((e = p.pprob.ensure((size_t)std::max<int64_t>(ptot, 1) * 4)) != cudaSuccess) return cuda_fail(e, "alloc pprob");
+  if ((e = p.iprob.ensure((size_t)std::max<int64_t>(itot, 1) * 4)) != cudaSuccess) return cuda_fail(e, "alloc iprob");
+  if ((e = p.offs.ensure((size_t)nb * 2 * 8)) != cudaSuccess) return cuda_fail(e, "alloc offs");
+  if ((e = p.pprob_sum.ensure((size_t)nb * (L + 2) * 8 * 4)) != cudaSuccess) return cuda_fail(e, "alloc psum");
+  if ((e = p.pprob_sumsum.ensure((size_t)nb * (L + 2) * 4)) != cudaSuccess) return cuda_fail(e, "alloc pss");
+  if ((e = p.iprob_sum.ensure((size_t)nb * L * 8 * 4)) != cudaSuccess) return cuda_fail(e, "alloc isum");
+  if ((e = p.of1.ensure((size_t)nb * L * 8 * 4)) != cudaSuccess) return cuda_fail(e, "alloc of1");
+  if ((e = p.dip.ensure((size_t)nb * (L + 2) * 4)) != cudaSuccess) return cuda_fail(e, "alloc dip");
+  if ((e = p.err.ensure((size_t)nb * 4)) != cudaSuccess) return cuda_fail(e, "alloc err");
+  std::vector<int64_t> offs(poff);
+  offs.insert(offs.end(), ioff.begin(), ioff.end());
+  cudaMemcpyAsync(p.offs.ptr, offs.data(), offs.size() * 8, cudaMemcpyHostToDevice, stream);
+  PhaseStore S;
+  S.pprob = p.pprob.as<float>();
+  S.pprob_off = p.offs.as<int64_t>();
+  S.pprob_sum = p.pprob_sum.as<float>();
+  S.pprob_sumsum = p.pprob_sumsum.as<float>();
+  S.iprob = p.iprob.as<float>();
+  S.iprob_off = p.offs.as<int64_t>() + nb;
+  S.iprob_sum = p.iprob_sum.as<float>();
+  S.of1 = p.of1.as<float>();
+  S.dip = p.dip.as<int32_t>();
+  S.err = p.err.as<int32_t>();
+  const int J = std::max(1, (Kmax + kPhaseThreads - 1) / kPhaseThreads);
+  if (launch_phase(J, d_tsel, nb, w.nstates.as<int32_t>(), w.hvar.as<uint32_t>(), w.WB, w.Kp, w.poly.as<int32_t>(),
+                   L, panel.cm, V, S, mc, cfg.seed, iteration, d_target_ids, stream) != GP_OK)
+    return (fail(GP_E_ARG, "phasing: too many states"), GP_E_ARG);
+  launch_phase_writeback(d_tsel, nb, w.poly.as<int32_t>(), w.polyidx.as<int32_t>(), L, V, S, mc, cfg.seed, iteration,
+                         d_target_ids, d_h0, d_h1, stream);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "phasing launch");
+  last_phase_nseg.assign(cnt.begin() + nb, cnt.begin() + 2 * nb);
   return GP_OK;
 }
 
@@ -276,10 +358,46 @@ int gp_impute_batch(gp_ctx* ctx, int32_t n, const int64_t* states_off, const uin
   if ((e = w.flat.ensure((size_t)n * L)) != cudaSuccess) return c.cuda_fail(e, "alloc flat");
   cudaMemcpyAsync(w.hl.ptr, hl, (size_t)n * 2 * L * 4, cudaMemcpyHostToDevice, c.stream);
   cudaMemcpyAsync(w.flat.ptr, flat, (size_t)n * L, cudaMemcpyHostToDevice, c.stream);
-  int rc = c.impute_device(n, off, st, w.hl.as<float>(), w.flat.as<uint8_t>(), w.hp.as<float>());
+  int rc = c.build_condsets(n, off, st);
+  if (rc != GP_OK) return rc;
+  rc = c.run_impute(w.hl.as<float>(), w.flat.as<uint8_t>(), w.hp.as<float>());
   if (rc != GP_OK) return rc;
   cudaMemcpyAsync(hp, w.hp.ptr, (size_t)n * 2 * L * 4, cudaMemcpyDeviceToHost, c.stream);
   if ((e = cudaStreamSynchronize(c.stream)) != cudaSuccess) return c.cuda_fail(e, "impute");
+  return GP_OK;
+}
+
+int gp_rephase_batch(gp_ctx* ctx, int32_t n, const int64_t* states_off, const uint32_t* states, uint8_t* h0,
+                     uint8_t* h1, const uint8_t* flat, int32_t iteration, const int32_t* target_ids) {
+  if (!ctx) return GP_E_ARG;
+  Context& c = *reinterpret_cast<Context*>(ctx);
+  if (n <= 0 || !states_off || !states || !h0 || !h1 || !flat) return (c.fail(GP_E_ARG, "rephase: bad argument"), GP_E_ARG);
+  const int L = c.panel.L;
+  std::vector<int64_t> off(states_off, states_off + n + 1);
+  std::vector<uint32_t> st(states, states + off[n]);
+  int rc = c.build_condsets(n, off, st);
+  if (rc != GP_OK) return rc;
+  gp::DevBuf& bh0 = c.scratch_h0;
+  gp::DevBuf& bh1 = c.scratch_h1;
+  gp::DevBuf& bfl = c.impute.flat;
+  gp::DevBuf& bid = c.scratch_ids;
+  cudaError_t e;
+  if ((e = bh0.ensure((size_t)n * L)) != cudaSuccess) return c.cuda_fail(e, "alloc h0");
+  if ((e = bh1.ensure((size_t)n * L)) != cudaSuccess) return c.cuda_fail(e, "alloc h1");
+  if ((e = bfl.ensure((size_t)n * L)) != cudaSuccess) return c.cuda_fail(e, "alloc flat");
+  if ((e = bid.ensure((size_t)n * 4)) != cudaSuccess) return c.cuda_fail(e, "alloc ids");
+  std::vector<int32_t> ids(n);
+  for (int i = 0; i < n; ++i) ids[i] = target_ids ? target_ids[i] : i;
+  cudaMemcpyAsync(bh0.ptr, h0, (size_t)n * L, cudaMemcpyHostToDevice, c.stream);
+  cudaMemcpyAsync(bh1.ptr, h1, (size_t)n * L, cudaMemcpyHostToDevice, c.stream);
+  cudaMemcpyAsync(bfl.ptr, flat, (size_t)n * L, cudaMemcpyHostToDevice, c.stream);
+  cudaMemcpyAsync(bid.ptr, ids.data(), (size_t)n * 4, cudaMemcpyHostToDevice, c.stream);
+  rc = c.run_phase(nullptr, {}, n, bh0.as<uint8_t>(), bh1.as<uint8_t>(), bfl.as<uint8_t>(), iteration,
+                   bid.as<int32_t>());
+  if (rc != GP_OK) return rc;
+  cudaMemcpyAsync(h0, bh0.ptr, (size_t)n * L, cudaMemcpyDeviceToHost, c.stream);
+  cudaMemcpyAsync(h1, bh1.ptr, (size_t)n * L, cudaMemcpyDeviceToHost, c.stream);
+  if ((e = cudaStreamSynchronize(c.stream)) != cudaSuccess) return c.cuda_fail(e, "rephase");
   return GP_OK;
 }
 

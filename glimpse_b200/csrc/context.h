@@ -28,14 +28,21 @@ struct Context {
   HostPanel host;
   DevPanel panel;
   ImputeWork impute;
+  PhaseWork phase;
+  DevBuf scratch_h0, scratch_h1, scratch_ids;
+  std::vector<int32_t> host_nstates;   // K per conditioning set of the current batch
+  std::vector<int32_t> impute_np;      // poly sites per conditioning set of the current batch
+  std::vector<int32_t> last_phase_nseg;
   std::vector<void*> owned;  // device allocations freed at destruction
 
   ~Context();
   Status fail(int code, const std::string& msg);
   int cuda_fail(cudaError_t e, const char* where);
   int create_panel(const gp_panel_desc& d);
-  int impute_device(int n, const std::vector<int64_t>& off, const std::vector<uint32_t>& states, const float* d_hl,
-                    const uint8_t* d_flat, float* d_hp);
+  int build_condsets(int n, const std::vector<int64_t>& off, const std::vector<uint32_t>& states);
+  int run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp);
+  int run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_host, int nb, uint8_t* d_h0, uint8_t* d_h1,
+                const uint8_t* d_flat, int iteration, const int32_t* d_target_ids);
 };
 
 }  // namespace gp

@@ -70,6 +70,16 @@ struct ImputeWork {
   DevBuf hl, hp, flat;
 };
 
+// Scratch of the phasing HMM.
+struct PhaseWork {
+  DevBuf rel, code, seg, miss, seg_start, counts;
+  DevBuf pprob, iprob, offs, pprob_sum, pprob_sumsum, iprob_sum, of1, dip, err;
+  std::vector<DevBuf*> all() {
+    return {&rel, &code, &seg, &miss, &seg_start, &counts, &pprob, &iprob, &offs, &pprob_sum, &pprob_sumsum,
+            &iprob_sum, &of1, &dip, &err};
+  }
+};
+
 // Model constants derived from gp_config the way the reference derives them
 // (conditioning_set.cpp:27-37, caller_initialise.cpp:150-153).
 struct ModelConst {

@@ -1,0 +1,615 @@
+// The 8-hypothesis phasing HMM with Gibbs phase resampling
+// (phase/src/models/phasing_hmm.{h,cpp}, rephaseHaplotypes :247-302).
+//
+// One block per diploid target. Thread `tid` owns states k = tid + 256*j and,
+// for each, the 8 hypothesis messages prob[k][0..7] in registers. Per-site
+// hypothesis sums (probSumH) are block reductions; SUMK is per state.
+// Segment-start messages (phasingProb) and flat-het messages (imputeProb) from
+// the backward pass are stored in global memory as [seg][k][8] rows.
+#include <cub/block/block_scan.cuh>
+
+#include "internal.h"
+#include "phase.h"
+
+namespace gp {
+
+namespace {
+
+constexpr int PT = kPhaseThreads;
+constexpr int NW = PT / kWarp;
+
+// ---------------------------------------------------------------------------
+// VAR list and segmentation (phasing_hmm.cpp:65-140)
+// ---------------------------------------------------------------------------
+template <int THREADS, int ITEMS>
+__global__ void k_build_vars(const int32_t* __restrict__ poly, const int32_t* __restrict__ npoly,
+                             const uint8_t* __restrict__ h0, const uint8_t* __restrict__ h1,
+                             const uint8_t* __restrict__ flat, const uint8_t* __restrict__ lq, int L,
+                             const int32_t* __restrict__ tsel, PhaseVars V) {
+  typedef cub::BlockScan<int, THREADS> Scan;
+  __shared__ typename Scan::TempStorage tmp;
+  __shared__ int carry[3];
+  const int b = blockIdx.x;
+  const int t = tsel ? tsel[b] : b;
+  const int np = npoly[t];
+  const int32_t* pl = poly + (size_t)t * L;
+  const uint8_t* H0 = h0 + (size_t)t * L;
+  const uint8_t* H1 = h1 + (size_t)t * L;
+  const uint8_t* FL = flat + (size_t)t * L;
+  int32_t* vrel = V.rel + (size_t)b * L;
+  uint8_t* vcode = V.code + (size_t)b * L;
+  int32_t* vseg = V.seg + (size_t)b * L;
+  int32_t* vmiss = V.miss + (size_t)b * L;
+  int32_t* sstart = V.seg_start + (size_t)b * (L + 2);
+  if (threadIdx.x < 3) carry[threadIdx.x] = 0;
+  __syncthreads();
+  for (int base = 0; base < np; base += THREADS * ITEMS) {
+    int isv[ITEMS], isph[ITEMS], isfh[ITEMS], code[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+      const int l = base + threadIdx.x * ITEMS + i;
+      isv[i] = isph[i] = isfh[i] = 0;
+      code[i] = 0;
+      if (l < np) {
+        const int s = pl[l];
+        const int a0 = H0[s], a1 = H1[s];
+        const bool nf = !FL[s] && !lq[s];
+        if (nf) {
+          isv[i] = 1;
+          if (a0 != a1) { isph[i] = 1; code[i] = 0; }
+          else code[i] = VT_HOM | (a0 << 3);
+        } else if (a0 != a1) {
+          isv[i] = 1;
+          isfh[i] = 1;
+          code[i] = VT_FLAT | (a0 << 3);
+        }
+      }
+    }
+    int exv[ITEMS], exh[ITEMS], exm[ITEMS];
+    int tv, th, tm;
+    Scan(tmp).ExclusiveSum(isv, exv, tv);
+    __syncthreads();
+    Scan(tmp).ExclusiveSum(isph, exh, th);
+    __syncthreads();
+    Scan(tmp).ExclusiveSum(isfh, exm, tm);
+    const int cv = carry[0], ch = carry[1], cmm = carry[2];
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+      const int l = base + threadIdx.x * ITEMS + i;
+      if (l < np && isv[i]) {
+        const int vi = cv + exv[i];
+        const int hc = ch + exh[i];  // peak hets before this entry
+        int c = code[i];
+        int seg;
+        if (isph[i]) {
+          c = hc % 3;  // VAR_TYP = n_het % 3
+          seg = hc / 3;
+          if (hc > 0 && hc % 3 == 0) sstart[seg] = vi;
+        } else {
+          seg = (hc > 0 ? hc - 1 : 0) / 3;
+        }
+        vrel[vi] = l;
+        vcode[vi] = (uint8_t)c;
+        vseg[vi] = seg;
+        vmiss[vi] = isfh[i] ? cmm + exm[i] : -1;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      carry[0] = cv + tv;
+      carry[1] = ch + th;
+      carry[2] = cmm + tm;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const int nv = carry[0], nh = carry[1], nm = carry[2];
+    const int nseg = (nh > 0 ? nh - 1 : 0) / 3 + 1;
+    sstart[0] = 0;
+    sstart[nseg] = nv;
+    V.nvar[b] = nv;
+    V.nseg[b] = nseg;
+    V.nmiss[b] = nm;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Block reduction of 8 values (one per hypothesis).
+// Within a warp a reduce-scatter leaves lane L with the warp sum of value
+// ((L>>4)&1)*4 + ((L>>3)&1)*2 + ((L>>2)&1); warps are then combined in order.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void block_sum8(float (&v)[8], float (*red)[NW][8], int& buf, float (&out)[8]) {
+  const int lane = threadIdx.x & 31;
+  float a[4], bb[2], c;
+  {
+    const bool up = lane & 16;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float send = up ? v[i] : v[i + 4];
+      const float keep = up ? v[i + 4] : v[i];
+      a[i] = __fadd_rn(keep, __shfl_xor_sync(0xffffffffu, send, 16));
+    }
+  }
+  {
+    const bool up = lane & 8;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const float send = up ? a[i] : a[i + 2];
+      const float keep = up ? a[i + 2] : a[i];
+      bb[i] = __fadd_rn(keep, __shfl_xor_sync(0xffffffffu, send, 8));
+    }
+  }
+  {
+    const bool up = lane & 4;
+    const float send = up ? bb[0] : bb[1];
+    const float keep = up ? bb[1] : bb[0];
+    c = __fadd_rn(keep, __shfl_xor_sync(0xffffffffu, send, 4));
+  }
+  c = __fadd_rn(c, __shfl_xor_sync(0xffffffffu, c, 2));
+  c = __fadd_rn(c, __shfl_xor_sync(0xffffffffu, c, 1));
+  const int warp = threadIdx.x >> 5;
+  if ((lane & 3) == 0) red[buf][warp][((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1)] = c;
+  __syncthreads();
+#pragma unroll
+  for (int h = 0; h < 8; ++h) {
+    float s = red[buf][0][h];
+#pragma unroll
+    for (int w = 1; w < NW; ++w) s = __fadd_rn(s, red[buf][w][h]);
+    out[h] = s;
+  }
+  buf ^= 1;
+}
+
+// horizontal_add of 8 lanes as the reference's AVX reduction orders it
+// (phasing_hmm.h:47-57): ((v0+v4)+(v1+v5)) + ((v2+v6)+(v3+v7)).
+__device__ __forceinline__ float hadd8(const float (&v)[8]) {
+  const float l0 = __fadd_rn(v[0], v[4]), l1 = __fadd_rn(v[1], v[5]);
+  const float l2 = __fadd_rn(v[2], v[6]), l3 = __fadd_rn(v[3], v[7]);
+  return __fadd_rn(__fadd_rn(l0, l1), __fadd_rn(l2, l3));
+}
+
+// Hypothesis allele at a het of type `typ` (ALLELE(HAP_NUMBER-h-1, 2-typ), phasing_hmm.h:45).
+__device__ __forceinline__ int hyp_allele(int h, int typ) { return ((7 - h) >> (2 - typ)) & 1; }
+
+__device__ __forceinline__ float transition(const double* __restrict__ cm, int prev, int next, const ModelConst& mc) {
+  const double d = mc.nrho * (cm[next] - cm[prev]);
+  double x = -expm1(d);
+  x = x < 1e-7 ? 1e-7 : (x > mc.one_l ? mc.one_l : x);
+  return (float)x;  // conditioning_set.h:101-105
+}
+
+struct PhaseShared {
+  float red[2][NW][8];
+  float sumH[8];
+  float sumT;
+  float hprobs[64];
+  float of1[8];
+  int dip;
+  int err;
+};
+
+// One site update: INIT / RUN / COLLAPSE of PEAK_HET, PEAK_HOM or FLAT_HET
+// (phasing_hmm.h:140-366), then the hypothesis sums.
+template <int J>
+__device__ __forceinline__ void site_update(float (&prob)[J][8], const float (&sumk)[J], const uint32_t (&w)[J],
+                                            int sh, int K, int tid, int typ, int alt, int mode, float yt, float nt,
+                                            const ModelConst& mc, float (&sumH)[8], float& sumT,
+                                            float (*red)[NW][8], int& buf) {
+  // mode: 0 INIT, 1 RUN, 2 COLLAPSE
+  const float Kf = (float)K;
+  float tF[8];
+  float ntp = 0.f;
+  if (mode != 0) {
+    const float sc = yt / __fmul_rn(Kf, sumT);
+#pragma unroll
+    for (int h = 0; h < 8; ++h) tF[h] = __fmul_rn(sumH[h], sc);
+    ntp = nt / sumT;
+  }
+  const float mism = mc.ed_phs / mc.ee_phs;
+  float part[8];
+#pragma unroll
+  for (int h = 0; h < 8; ++h) part[h] = 0.f;
+  if (typ == VT_FLAT && mode == 0) {
+    const float v = 1.0f / (float)(8u * (unsigned)K);
+#pragma unroll
+    for (int j = 0; j < J; ++j)
+#pragma unroll
+      for (int h = 0; h < 8; ++h) prob[j][h] = v;
+#pragma unroll
+    for (int h = 0; h < 8; ++h) sumH[h] = 0.125f;
+    sumT = 1.0f;
+    return;
+  }
+#pragma unroll
+  for (int j = 0; j < J; ++j) {
+    const int k = tid + j * PT;
+    if (k >= K) continue;
+    const int bit = (w[j] >> sh) & 1u;
+#pragma unroll
+    for (int h = 0; h < 8; ++h) {
+      float base;
+      if (mode == 0) base = 1.0f;
+      else if (mode == 1) base = fmaf(prob[j][h], ntp, tF[h]);
+      else base = fmaf(sumk[j], ntp, tF[h]);
+      float v;
+      if (typ < 3) {
+        const float e = (bit == hyp_allele(h, typ)) ? mc.ee_phs : mc.ed_phs;
+        v = (mode == 0) ? e : __fmul_rn(base, e);
+      } else if (typ == VT_HOM) {
+        if (mode == 0) v = (bit != alt) ? mism : 1.0f;
+        else v = (bit != alt) ? __fmul_rn(base, mism) : base;
+      } else {
+        v = base;  // flat het: no emission
+      }
+      prob[j][h] = v;
+      part[h] = __fadd_rn(part[h], v);
+    }
+  }
+  block_sum8(part, red, buf, sumH);
+  sumT = hadd8(sumH);
+}
+
+template <int J>
+__global__ void __launch_bounds__(PT) k_phase(const int32_t* __restrict__ tsel, const int32_t* __restrict__ nstates,
+                                              const uint32_t* __restrict__ hvar, int WB, int Kp,
+                                              const int32_t* __restrict__ poly, int L,
+                                              const double* __restrict__ cm, PhaseVars V, PhaseStore S,
+                                              ModelConst mc, uint64_t seed, int iteration,
+                                              const int32_t* __restrict__ target_ids) {
+  __shared__ PhaseShared sm;
+  int buf = 0;
+  const int b = blockIdx.x;
+  const int t = tsel ? tsel[b] : b;
+  const int K = nstates[t];
+  const int nv = V.nvar[b];
+  const int nseg = V.nseg[b];
+  const int tid = threadIdx.x;
+  if (tid == 0) sm.err = 0;
+  const uint32_t* hv = hvar + (size_t)t * WB * Kp;
+  const int32_t* vrel = V.rel + (size_t)b * L;
+  const uint8_t* vcode = V.code + (size_t)b * L;
+  const int32_t* vseg = V.seg + (size_t)b * L;
+  const int32_t* vmiss = V.miss + (size_t)b * L;
+  const int32_t* sstart = V.seg_start + (size_t)b * (L + 2);
+  const int32_t* pl = poly + (size_t)t * L;
+  float* PP = S.pprob + S.pprob_off[b];            // [nseg][K][8]
+  float* PPS = S.pprob_sum + (size_t)b * (L + 2) * 8;  // [nseg][8]
+  float* PPSS = S.pprob_sumsum + (size_t)b * (L + 2);  // [nseg]
+  float* IP = S.iprob + S.iprob_off[b];            // [nmiss][K][8]
+  float* IPS = S.iprob_sum + (size_t)b * L * 8;     // [nmiss][8]
+  float* OF1 = S.of1 + (size_t)b * L * 8;           // [nmiss][8]
+  int32_t* dip = S.dip + (size_t)b * (L + 2);
+  const uint32_t rng_target = target_ids ? (uint32_t)target_ids[b] : (uint32_t)t;
+
+  float prob[J][8];
+  float sumk[J];
+  uint32_t w[J];
+  float sumH[8];
+  float sumT = 0.f;
+#pragma unroll
+  for (int j = 0; j < J; ++j) sumk[j] = 0.f;
+  int loaded_block = -1;
+
+  auto load_bits = [&](int l) {
+    const int blk = l >> 5;
+    if (blk != loaded_block) {
+      loaded_block = blk;
+#pragma unroll
+      for (int j = 0; j < J; ++j) {
+        const int k = tid + j * PT;
+        w[j] = (k < K) ? hv[(size_t)blk * Kp + k] : 0u;
+      }
+    }
+  };
+  auto do_sumk = [&]() {
+#pragma unroll
+    for (int j = 0; j < J; ++j) sumk[j] = hadd8(prob[j]);
+  };
+
+  // ---------------- backward (phasing_hmm.cpp:193-245) ----------------
+  for (int i = nv - 1; i >= 0; --i) {
+    const int l = vrel[i];
+    load_bits(l);
+    const int code = vcode[i];
+    const int typ = code & 7, alt = (code >> 3) & 1;
+    const int seg = vseg[i];
+    const int locus = i - sstart[seg];
+    const int seglen = sstart[seg + 1] - sstart[seg];
+    float yt = 0.f;
+    if (i < nv - 1) yt = transition(cm, pl[l], pl[vrel[i + 1]], mc);
+    const float nt = 1.0f - yt;
+    const int mode = (i == nv - 1) ? 0 : ((locus != seglen - 1) ? 1 : 2);
+    site_update<J>(prob, sumk, w, l & 31, K, tid, typ, alt, mode, yt, nt, mc, sumH, sumT, sm.red, buf);
+    if (locus == 0) {
+      do_sumk();
+      float* dst = PP + (size_t)seg * K * 8;
+#pragma unroll
+      for (int j = 0; j < J; ++j) {
+        const int k = tid + j * PT;
+        if (k < K) {
+          float4* d4 = reinterpret_cast<float4*>(dst + (size_t)k * 8);
+          d4[0] = make_float4(prob[j][0], prob[j][1], prob[j][2], prob[j][3]);
+          d4[1] = make_float4(prob[j][4], prob[j][5], prob[j][6], prob[j][7]);
+        }
+      }
+      if (tid < 8) PPS[seg * 8 + tid] = sumH[tid];
+      if (tid == 0) PPSS[seg] = sumT;
+    }
+    if (typ == VT_FLAT) {
+      const int m = vmiss[i];
+      float* dst = IP + (size_t)m * K * 8;
+#pragma unroll
+      for (int j = 0; j < J; ++j) {
+        const int k = tid + j * PT;
+        if (k < K) {
+          float4* d4 = reinterpret_cast<float4*>(dst + (size_t)k * 8);
+          d4[0] = make_float4(prob[j][0], prob[j][1], prob[j][2], prob[j][3]);
+          d4[1] = make_float4(prob[j][4], prob[j][5], prob[j][6], prob[j][7]);
+        }
+      }
+      if (tid < 8) IPS[m * 8 + tid] = sumH[tid];
+    }
+  }
+  __syncthreads();
+
+  // ---------------- first diplotype draw (phasing_hmm.cpp:249-256) ----------------
+  if (tid == 0) {
+    int d0 = 7;
+    if (nv > 0) {
+      float dp[8];
+      float sd = 0.f;
+      for (int d = 0; d < 8; ++d) {
+        dp[d] = __fmul_rn(PPS[d] / PPSS[0], PPS[7 - d] / PPSS[0]);
+        sd = __fadd_rn(sd, dp[d]);
+      }
+      const float u = __fmul_rn(canonical_float(stream_word(seed, RNG_PHASE, iteration, rng_target, 0)), sd);
+      float cs = dp[0];
+      d0 = 7;
+      for (int d = 0; d < 7; ++d) {
+        if (u <= cs) { d0 = d; break; }
+        cs = __fadd_rn(cs, dp[d + 1]);
+      }
+    }
+    dip[0] = d0;
+    sm.dip = d0;
+  }
+  __syncthreads();
+
+  // ---------------- forward (phasing_hmm.cpp:142-191) ----------------
+  loaded_block = -1;
+  for (int i = 0; i < nv; ++i) {
+    const int l = vrel[i];
+    load_bits(l);
+    const int code = vcode[i];
+    const int typ = code & 7, alt = (code >> 3) & 1;
+    const int seg = vseg[i];
+    const int locus = i - sstart[seg];
+    const int seglen = sstart[seg + 1] - sstart[seg];
+    float yt = 0.f;
+    if (i) yt = transition(cm, pl[vrel[i - 1]], pl[l], mc);
+    const float nt = 1.0f - yt;
+    const int mode = (i == 0) ? 0 : ((locus != 0) ? 1 : 2);
+    site_update<J>(prob, sumk, w, l & 31, K, tid, typ, alt, mode, yt, nt, mc, sumH, sumT, sm.red, buf);
+    const bool seg_end = (locus == seglen - 1);
+    if (seg_end) do_sumk();
+    if (seg_end && i != nv - 1) {
+      // TRANS_HAP (phasing_hmm.h:376-397)
+      const float yt2 = transition(cm, pl[l], pl[vrel[i + 1]], mc);
+      const float nt2 = 1.0f - yt2;
+      const float fact2 = nt2 / sumT;
+      const float* nxt = PP + (size_t)(seg + 1) * K * 8;
+      float sumHP = 0.f;
+#pragma unroll
+      for (int h1 = 0; h1 < 8; ++h1) {
+        const float fact1 = __fmul_rn(sumH[h1] / sumT, yt2) / (float)K;
+        float acc[8];
+#pragma unroll
+        for (int h2 = 0; h2 < 8; ++h2) acc[h2] = 0.f;
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+          const int k = tid + j * PT;
+          if (k < K) {
+            const float p0 = fmaf(prob[j][h1], fact2, fact1);
+            const float4* s4 = reinterpret_cast<const float4*>(nxt + (size_t)k * 8);
+            const float4 x = s4[0], y = s4[1];
+            acc[0] = fmaf(p0, x.x, acc[0]); acc[1] = fmaf(p0, x.y, acc[1]);
+            acc[2] = fmaf(p0, x.z, acc[2]); acc[3] = fmaf(p0, x.w, acc[3]);
+            acc[4] = fmaf(p0, y.x, acc[4]); acc[5] = fmaf(p0, y.y, acc[5]);
+            acc[6] = fmaf(p0, y.z, acc[6]); acc[7] = fmaf(p0, y.w, acc[7]);
+          }
+        }
+        float tot[8];
+        block_sum8(acc, sm.red, buf, tot);
+        if (tid == 0)
+#pragma unroll
+          for (int h2 = 0; h2 < 8; ++h2) sm.hprobs[h1 * 8 + h2] = tot[h2];
+        sumHP = __fadd_rn(sumHP, hadd8(tot));
+      }
+      // SAMPLE_DIP (phasing_hmm.h:400-411)
+      if (tid == 0) {
+        const bool bad1 = isnan(sumHP) || isinf(sumHP) || sumHP < 1.17549435e-38f;
+        const int prev = sm.dip;
+        float dp[8];
+        float sd = 0.f;
+        for (int d = 0; d < 8; ++d) {
+          dp[d] = __fmul_rn(sm.hprobs[prev * 8 + d] / sumHP, sm.hprobs[(7 - prev) * 8 + (7 - d)] / sumHP);
+          sd = __fadd_rn(sd, dp[d]);
+        }
+        const bool bad2 = isnan(sd) || isinf(sd) || sd < 1.17549435e-38f;
+        int nd = prev;
+        if (bad1 || bad2) {
+          sm.err = 1;
+        } else {
+          const float u = __fmul_rn(canonical_float(stream_word(seed, RNG_PHASE, iteration, rng_target,
+                                                                (uint64_t)(seg + 1))), sd);
+          float cs = dp[0];
+          nd = 7;
+          for (int d = 0; d < 7; ++d) {
+            if (u <= cs) { nd = d; break; }
+            cs = __fadd_rn(cs, dp[d + 1]);
+          }
+        }
+        dip[seg + 1] = nd;
+        sm.dip = nd;
+      }
+      __syncthreads();
+    }
+    if (typ == VT_FLAT) {
+      // IMPUTE_FLAT_HET (phasing_hmm.h:414-447)
+      const int m = vmiss[i];
+      const float* src = IP + (size_t)m * K * 8;
+      float sR[8], sL[8];
+#pragma unroll
+      for (int h = 0; h < 8; ++h) {
+        sR[h] = 1.0f / IPS[m * 8 + h];
+        sL[h] = 1.0f / sumH[h];
+      }
+      float s0[8], s1[8];
+#pragma unroll
+      for (int h = 0; h < 8; ++h) s0[h] = s1[h] = 0.f;
+#pragma unroll
+      for (int j = 0; j < J; ++j) {
+        const int k = tid + j * PT;
+        if (k < K) {
+          const int bit = (w[j] >> (l & 31)) & 1u;
+          const float4* s4 = reinterpret_cast<const float4*>(src + (size_t)k * 8);
+          const float4 x = s4[0], y = s4[1];
+          const float ip[8] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
+#pragma unroll
+          for (int h = 0; h < 8; ++h) {
+            const float p1 = __fmul_rn(ip[h], sR[h]);
+            const float p2 = __fmul_rn(prob[j][h], sL[h]);
+            if (bit) s1[h] = fmaf(p1, p2, s1[h]); else s0[h] = fmaf(p1, p2, s0[h]);
+          }
+        }
+      }
+      float t0[8], t1[8];
+      block_sum8(s0, sm.red, buf, t0);
+      block_sum8(s1, sm.red, buf, t1);
+      if (tid < 8) {
+        const float r = t1[tid] / __fadd_rn(t0[tid], t1[tid]);
+        OF1[m * 8 + tid] = fmaxf(0.0f, fminf(1.0f, r));
+      }
+    }
+  }
+  if (tid == 0) S.err[b] = sm.err;
+}
+
+// Allele write-back for peak and flat hets (phasing_hmm.cpp:260-292).
+__global__ void k_phase_writeback(const int32_t* __restrict__ tsel, const int32_t* __restrict__ poly, int L,
+                                  PhaseVars V, PhaseStore S, ModelConst mc, uint64_t seed, int iteration,
+                                  const int32_t* __restrict__ target_ids, uint8_t* __restrict__ h0,
+                                  uint8_t* __restrict__ h1) {
+  const int b = blockIdx.y;
+  const int t = tsel ? tsel[b] : b;
+  const int nv = V.nvar[b];
+  const int nseg = V.nseg[b];
+  const uint32_t rng_target = target_ids ? (uint32_t)target_ids[b] : (uint32_t)t;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x) {
+    const int code = V.code[(size_t)b * L + i];
+    const int typ = code & 7;
+    if (typ == VT_HOM) continue;
+    const int l = V.rel[(size_t)b * L + i];
+    const int s = poly[(size_t)t * L + l];
+    const int seg = V.seg[(size_t)b * L + i];
+    const int i0 = S.dip[(size_t)b * (L + 2) + seg];
+    const int i1 = 7 - i0;
+    if (typ < 3) {
+      h0[(size_t)t * L + s] = (uint8_t)hyp_allele(i0, typ);
+      h1[(size_t)t * L + s] = (uint8_t)hyp_allele(i1, typ);
+    } else {
+      const int m = V.miss[(size_t)b * L + i];
+      const float* of = S.of1 + ((size_t)b * L + m) * 8;
+      const float h0a0 = 1.0f - of[i0], h0a1 = of[i0];
+      const float h1a0 = 1.0f - of[i1], h1a1 = of[i1];
+      float p01 = __fmul_rn(fmaf(h0a0, mc.ee_phs, __fmul_rn(h0a1, mc.ed_phs)),
+                            fmaf(h1a1, mc.ee_phs, __fmul_rn(h1a0, mc.ed_phs)));
+      float p10 = __fmul_rn(fmaf(h0a1, mc.ee_phs, __fmul_rn(h0a0, mc.ed_phs)),
+                            fmaf(h1a0, mc.ee_phs, __fmul_rn(h1a1, mc.ed_phs)));
+      float sum = __fadd_rn(p01, p10);
+      p01 = fminf(fmaxf(p01 / sum, 0.0f), 1.0f);
+      p10 = fminf(fmaxf(p10 / sum, 0.0f), 1.0f);
+      sum = __fadd_rn(p01, p10);
+      const float u = canonical_float(stream_word(seed, RNG_PHASE, iteration, rng_target, (uint64_t)(nseg + m)));
+      const bool rf = __dmul_rn((double)u, (double)sum) < (double)p01;
+      h0[(size_t)t * L + s] = (uint8_t)(!rf);  // H0 written twice, H1 untouched (phasing_hmm.cpp:283-284)
+    }
+  }
+}
+
+// Shuffle of hets at monomorphic sites (phasing_hmm.cpp:293-301): the m-th such
+// het draws word nseg + nmiss + m of the target's phasing stream.
+template <int THREADS, int ITEMS>
+__global__ void k_mono_shuffle(const int32_t* __restrict__ tsel, const int32_t* __restrict__ polyidx, int L,
+                               PhaseVars V, uint64_t seed, int iteration, const int32_t* __restrict__ target_ids,
+                               uint8_t* __restrict__ h0, uint8_t* __restrict__ h1) {
+  typedef cub::BlockScan<int, THREADS> Scan;
+  __shared__ typename Scan::TempStorage tmp;
+  __shared__ int carry;
+  const int b = blockIdx.x;
+  const int t = tsel ? tsel[b] : b;
+  const uint32_t rng_target = target_ids ? (uint32_t)target_ids[b] : (uint32_t)t;
+  const uint64_t base_word = (uint64_t)V.nseg[b] + (uint64_t)V.nmiss[b];
+  uint8_t* H0 = h0 + (size_t)t * L;
+  uint8_t* H1 = h1 + (size_t)t * L;
+  const int32_t* pi = polyidx + (size_t)t * L;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < L; base += THREADS * ITEMS) {
+    int v[ITEMS], ex[ITEMS], tot;
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+      const int s = base + threadIdx.x * ITEMS + i;
+      v[i] = (s < L && pi[s] < 0 && H0[s] != H1[s]) ? 1 : 0;
+    }
+    Scan(tmp).ExclusiveSum(v, ex, tot);
+    const int c = carry;
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+      if (!v[i]) continue;
+      const int s = base + threadIdx.x * ITEMS + i;
+      const float u = canonical_float(stream_word(seed, RNG_PHASE, iteration, rng_target, base_word + c + ex[i]));
+      const bool rf = u < 0.5f;
+      H0[s] = (uint8_t)rf;
+      H1[s] = (uint8_t)!rf;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) carry = c + tot;
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+void launch_build_vars(const int32_t* tsel, int nb, const int32_t* poly, const int32_t* npoly, const uint8_t* h0,
+                       const uint8_t* h1, const uint8_t* flat, const uint8_t* lq, int L, PhaseVars V,
+                       cudaStream_t s) {
+  k_build_vars<512, 8><<<nb, 512, 0, s>>>(poly, npoly, h0, h1, flat, lq, L, tsel, V);
+}
+
+int launch_phase(int J, const int32_t* tsel, int nb, const int32_t* nstates, const uint32_t* hvar, int WB, int Kp,
+                 const int32_t* poly, int L, const double* cm, PhaseVars V, PhaseStore S, const ModelConst& mc,
+                 uint64_t seed, int iteration, const int32_t* target_ids, cudaStream_t s) {
+  switch (J) {
+    case 1: k_phase<1><<<nb, PT, 0, s>>>(tsel, nstates, hvar, WB, Kp, poly, L, cm, V, S, mc, seed, iteration, target_ids); break;
+    case 2: k_phase<2><<<nb, PT, 0, s>>>(tsel, nstates, hvar, WB, Kp, poly, L, cm, V, S, mc, seed, iteration, target_ids); break;
+    case 3: k_phase<3><<<nb, PT, 0, s>>>(tsel, nstates, hvar, WB, Kp, poly, L, cm, V, S, mc, seed, iteration, target_ids); break;
+    case 4: k_phase<4><<<nb, PT, 0, s>>>(tsel, nstates, hvar, WB, Kp, poly, L, cm, V, S, mc, seed, iteration, target_ids); break;
+    case 5: k_phase<5><<<nb, PT, 0, s>>>(tsel, nstates, hvar, WB, Kp, poly, L, cm, V, S, mc, seed, iteration, target_ids); break;
+    case 6: k_phase<6><<<nb, PT, 0, s>>>(tsel, nstates, hvar, WB, Kp, poly, L, cm, V, S, mc, seed, iteration, target_ids); break;
+    case 7: k_phase<7><<<nb, PT, 0, s>>>(tsel, nstates, hvar, WB, Kp, poly, L, cm, V, S, mc, seed, iteration, target_ids); break;
+    case 8: k_phase<8><<<nb, PT, 0, s>>>(tsel, nstates, hvar, WB, Kp, poly, L, cm, V, S, mc, seed, iteration, target_ids); break;
+    default: return GP_E_ARG;
+  }
+  return GP_OK;
+}
+
+void launch_phase_writeback(const int32_t* tsel, int nb, const int32_t* poly, const int32_t* polyidx, int L,
+                            PhaseVars V, PhaseStore S, const ModelConst& mc, uint64_t seed, int iteration,
+                            const int32_t* target_ids, uint8_t* h0, uint8_t* h1, cudaStream_t s) {
+  dim3 g(64, nb);
+  k_phase_writeback<<<g, 256, 0, s>>>(tsel, poly, L, V, S, mc, seed, iteration, target_ids, h0, h1);
+  k_mono_shuffle<512, 8><<<nb, 512, 0, s>>>(tsel, polyidx, L, V, seed, iteration, target_ids, h0, h1);
+}
+
+}  // namespace gp

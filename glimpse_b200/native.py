@@ -135,3 +135,18 @@ class Context:
         self._check(self.lib.gp_impute_batch(self.h, n, _p(off, C.c_int64), _p(st, C.c_uint32), _p(hl, C.c_float),
                                              _p(flat, C.c_uint8), _p(hp, C.c_float)))
         return hp
+
+    def rephase_batch(self, states_list, h0, h1, flat, iteration, target_ids=None):
+        """phasing_hmm::rephaseHaplotypes for len(states_list) diploid targets."""
+        n = len(states_list)
+        off = np.zeros(n + 1, np.int64)
+        off[1:] = np.cumsum([len(s) for s in states_list])
+        st = np.ascontiguousarray(np.concatenate([np.asarray(s, np.uint32) for s in states_list]), np.uint32)
+        h0 = np.array(h0, np.uint8, copy=True).reshape(n, self.L)
+        h1 = np.array(h1, np.uint8, copy=True).reshape(n, self.L)
+        flat = np.ascontiguousarray(flat, np.uint8).reshape(n, self.L)
+        ids = None if target_ids is None else np.ascontiguousarray(target_ids, np.int32)
+        self._check(self.lib.gp_rephase_batch(self.h, n, _p(off, C.c_int64), _p(st, C.c_uint32), _p(h0, C.c_uint8),
+                                              _p(h1, C.c_uint8), _p(flat, C.c_uint8), iteration,
+                                              _p(ids, C.c_int32)))
+        return h0, h1

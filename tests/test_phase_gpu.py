@@ -1,0 +1,45 @@
+"""Phasing HMM parity: GPU rephase vs the reference's
+phasing_hmm::rephaseHaplotypes (phasing_hmm.cpp:247-302) on identical
+haplotypes, flat flags, conditioning sets and random streams. The outputs are
+discrete (sampled diplotypes and alleles) and must be identical."""
+import numpy as np
+import pytest
+
+from conftest import ref_oracle_or_skip
+
+
+def _noisy_haps(rng, truth, p=0.03):
+    h = truth.copy()
+    flip = rng.random(h.shape) < p
+    h[flip] ^= 1
+    return h
+
+
+@pytest.mark.gpu
+def test_rephase_matches_reference(small_workload):
+    O = ref_oracle_or_skip()
+    from glimpse_b200 import native
+    w = small_workload
+    P, T = w.panel, w.targets
+    orc = O.RefOracle(P, T, kinit=200, kpbwt=150)
+    ctx = native.Context(P)
+    rng = np.random.default_rng(5)
+    cases = []
+    for t in range(T.n):
+        for K in (6, 64, 257, 520):
+            s = np.sort(rng.choice(P.n_ref_haps, size=K, replace=False)).astype(np.uint32)
+            h0 = _noisy_haps(rng, T.truth[t, 0])
+            h1 = _noisy_haps(rng, T.truth[t, 1])
+            cases.append((s, h0, h1, T.flat[t], t))
+    it = 3
+    refs = [orc.rephase(s, h0, h1, fl, it, tid) for (s, h0, h1, fl, tid) in cases]
+    g0, g1 = ctx.rephase_batch([c[0] for c in cases], np.stack([c[1] for c in cases]),
+                               np.stack([c[2] for c in cases]), np.stack([c[3] for c in cases]), it,
+                               target_ids=[c[4] for c in cases])
+    bad = []
+    for i, (r0, r1, dip) in enumerate(refs):
+        n0 = int((g0[i] != r0).sum())
+        n1 = int((g1[i] != r1).sum())
+        if n0 or n1:
+            bad.append((i, n0, n1, len(dip)))
+    assert not bad, f"haplotype mismatches (case, #H0, #H1, nseg): {bad}"
