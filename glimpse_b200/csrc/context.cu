@@ -8,6 +8,7 @@
 
 #include "context.h"
 #include "phase.h"
+#include "genotype.h"
 
 namespace gp {
 
@@ -118,6 +119,25 @@ int Context::create_panel(const gp_panel_desc& d) {
   if ((e = upload(&P.shap_off, host.shap_off.data(), N + 1, owned)) != cudaSuccess) return cuda_fail(e, "shap_off");
   if ((e = upload(&P.shap_sites, host.shap_sites.data(), (size_t)nnz, owned)) != cudaSuccess)
     return cuda_fail(e, "shap_sites");
+  // SvarRef (haplotype_set::transposeRareRef, haplotype_set.cpp:201-214)
+  host.svar_off.assign(L + 1, 0);
+  for (int64_t j = 0; j < nnz; ++j) host.svar_off[host.shap_sites[j] + 1]++;
+  for (int l = 0; l < L; ++l) host.svar_off[l + 1] += host.svar_off[l];
+  host.svar_haps.assign(nnz, 0);
+  {
+    std::vector<int64_t> fill(host.svar_off.begin(), host.svar_off.end() - 1);
+    for (int h = 0; h < N; ++h)
+      for (int64_t j = host.shap_off[h]; j < host.shap_off[h + 1]; ++j) host.svar_haps[fill[host.shap_sites[j]]++] = h;
+  }
+  host.common_sites.clear();
+  host.max_rare_mac = 0;
+  for (int l = 0; l < L; ++l) {
+    if (host.common[l]) host.common_sites.push_back(l);
+    else host.max_rare_mac = std::max<int>(host.max_rare_mac, (int)std::min(host.cref[l], host.calt[l]));
+  }
+  if ((e = upload(&P.svar_off, host.svar_off.data(), L + 1, owned)) != cudaSuccess) return cuda_fail(e, "svar_off");
+  if ((e = upload(&P.svar_haps, host.svar_haps.data(), (size_t)nnz, owned)) != cudaSuccess)
+    return cuda_fail(e, "svar_haps");
   if ((e = upload(&P.refT, (const uint32_t*)nullptr, (size_t)N * P.W, owned)) != cudaSuccess)
     return cuda_fail(e, "refT");
   if (nc > 0) {
@@ -134,7 +154,20 @@ int Context::create_panel(const gp_panel_desc& d) {
   } else {
     cudaMemsetAsync(P.refT, 0, sizeof(uint32_t) * N * P.W, stream);
   }
-  return GP_OK;
+  // Sparse PBWT: supplied with the panel (binary panel format) or built here.
+  if (d.ypacked && d.asmall_off && d.asmall_idx) {
+    sparse.ypacked.assign(d.ypacked, d.ypacked + d.ypacked_len);
+    sparse.asmall_off.assign(d.asmall_off, d.asmall_off + nchq + 2);
+    sparse.asmall.assign(d.asmall_idx, d.asmall_idx + sparse.asmall_off[nchq + 1]);
+  } else {
+    build_sparse_pbwt(N, L, host.lq.data(), host.common.data(), host.major.data(), host.cref.data(),
+                      host.calt.data(), host.hvar.data(), host.svar_off.data(), host.svar_haps.data(), sparse);
+  }
+  float tab[256];
+  unphred_table(tab);
+  if ((e = upload_unphred(tab)) != cudaSuccess) return cuda_fail(e, "unphred");
+  if ((e = upload_unphred_init(tab)) != cudaSuccess) return cuda_fail(e, "unphred");
+  return pbwt_prepare_panel();
 }
 
 Context::~Context() {
@@ -146,6 +179,8 @@ Context::~Context() {
   impute.alpha.release(); impute.alpha_off.release();
   impute.hl.release(); impute.hp.release(); impute.flat.release();
   for (DevBuf* b : phase.all()) b->release();
+  for (DevBuf* b : tw.all()) b->release();
+  scratch_h0.release(); scratch_h1.release(); scratch_ids.release();
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -398,6 +433,18 @@ int gp_rephase_batch(gp_ctx* ctx, int32_t n, const int64_t* states_off, const ui
   cudaMemcpyAsync(h0, bh0.ptr, (size_t)n * L, cudaMemcpyDeviceToHost, c.stream);
   cudaMemcpyAsync(h1, bh1.ptr, (size_t)n * L, cudaMemcpyDeviceToHost, c.stream);
   if ((e = cudaStreamSynchronize(c.stream)) != cudaSuccess) return c.cuda_fail(e, "rephase");
+  return GP_OK;
+}
+
+int gp_sparse_pbwt_get(gp_ctx* ctx, uint8_t* ypacked, int64_t* ypacked_len, int64_t* asmall_off,
+                       int32_t* asmall_idx, int64_t* asmall_len) {
+  if (!ctx) return GP_E_ARG;
+  Context& c = *reinterpret_cast<Context*>(ctx);
+  if (ypacked_len) *ypacked_len = (int64_t)c.sparse.ypacked.size();
+  if (asmall_len) *asmall_len = (int64_t)c.sparse.asmall.size();
+  if (ypacked) std::memcpy(ypacked, c.sparse.ypacked.data(), c.sparse.ypacked.size());
+  if (asmall_off) std::memcpy(asmall_off, c.sparse.asmall_off.data(), c.sparse.asmall_off.size() * 8);
+  if (asmall_idx) std::memcpy(asmall_idx, c.sparse.asmall.data(), c.sparse.asmall.size() * 4);
   return GP_OK;
 }
 

@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "internal.h"
+#include "select.h"
 
 namespace gp {
 
@@ -16,7 +17,34 @@ struct HostPanel {
   std::vector<uint8_t> hvar;
   std::vector<int64_t> shap_off;
   std::vector<int32_t> shap_sites;
+  std::vector<int64_t> svar_off;    // SvarRef: per rare site, carriers of the non-major allele
+  std::vector<int32_t> svar_haps;
+  std::vector<int32_t> common_sites;  // common2tot
+  std::vector<float> cm_pos;
+  int max_rare_mac = 0;
 };
+
+// Target batch state (genotype_set + the per-target-haplotype PBWT bookkeeping).
+struct TargetWork {
+  int n = 0;
+  std::vector<int32_t> ploidy_h, kpbwt_h, diploid;
+  std::vector<int32_t> hap_target, hap_which, target_hap0, target_nhap;
+  DevBuf gl, flat, ploidy, dip_list;
+  DevBuf h0, h1, hl, hp0, hp1;
+  DevBuf gp0, gp1, gpflags, ds, gt0, gt1;
+  DevBuf sind, nsind, bitmap;
+  DevBuf d_hap_target, d_hap_which, d_target_hap0, d_target_nhap, d_kpbwt, tar_hap, d_grp;
+  DevBuf push_key, push_id, push_cnt, stored_bits, start_idx, overflow;
+  int stored_cnt = 0;
+  bool finalized = false;
+  std::vector<DevBuf*> all() {
+    return {&gl, &flat, &ploidy, &dip_list, &h0, &h1, &hl, &hp0, &hp1, &gp0, &gp1, &gpflags, &ds, &gt0, &gt1,
+            &sind, &nsind, &bitmap, &d_hap_target, &d_hap_which, &d_target_hap0, &d_target_nhap, &d_kpbwt,
+            &tar_hap, &d_grp, &push_key, &push_id, &push_cnt, &stored_bits, &start_idx, &overflow};
+  }
+};
+
+void unphred_table(float* out);
 
 ModelConst model_constants(const gp_config& c, int n_ref_haps);
 
@@ -33,6 +61,14 @@ struct Context {
   std::vector<int32_t> host_nstates;   // K per conditioning set of the current batch
   std::vector<int32_t> impute_np;      // poly sites per conditioning set of the current batch
   std::vector<int32_t> last_phase_nseg;
+  TargetWork tw;
+  SparsePbwt sparse;
+  DevPbwt pbwt;
+  bool pbwt_active = false;
+  float pbwt_modulo = 0.1f;
+  std::vector<int32_t> pbwt_grp;
+  int tw_push_cap = 4096;
+  float stage_ms[5] = {0, 0, 0, 0, 0};
   std::vector<void*> owned;  // device allocations freed at destruction
 
   ~Context();
@@ -41,6 +77,15 @@ struct Context {
   int create_panel(const gp_panel_desc& d);
   int build_condsets(int n, const std::vector<int64_t>& off, const std::vector<uint32_t>& states);
   int run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp);
+  int set_targets(int n, const uint8_t* gl, const uint8_t* flat, const int32_t* ploidy, const int32_t* kp);
+  int build_condsets_device(int n, int Kp);
+  int select_states(int stage, int iteration, int& Kp);
+  int iteration(int stage, int iteration);
+  int finalize();
+  int pbwt_prepare_panel();
+  int pbwt_prepare_targets();
+  int pbwt_select_states(int stage, int iteration, int Kp);
+  int pbwt_states_get(int target, int32_t* counts, int32_t* states, int cap);
   int run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_host, int nb, uint8_t* d_h0, uint8_t* d_h1,
                 const uint8_t* d_flat, int iteration, const int32_t* d_target_ids);
 };

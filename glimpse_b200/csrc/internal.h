@@ -58,6 +58,8 @@ struct DevPanel {
   int64_t* shap_off = nullptr;     // [N+1]
   int32_t* shap_sites = nullptr;   // rare sites carrying the non-major allele, per haplotype
   int64_t shap_nnz = 0;
+  int64_t* svar_off = nullptr;     // [L+1] SvarRef CSR
+  int32_t* svar_haps = nullptr;
 };
 
 // Per-batch scratch for the imputation path (sized for n haplotypes).

@@ -262,7 +262,6 @@ __global__ void __launch_bounds__(PT) k_phase(const int32_t* __restrict__ tsel, 
   const int t = tsel ? tsel[b] : b;
   const int K = nstates[t];
   const int nv = V.nvar[b];
-  const int nseg = V.nseg[b];
   const int tid = threadIdx.x;
   if (tid == 0) sm.err = 0;
   const uint32_t* hv = hvar + (size_t)t * WB * Kp;

@@ -21,7 +21,7 @@ EXPORTS = [
     "gp_config_defaults", "gp_ctx_create", "gp_ctx_destroy", "gp_last_error", "gp_targets_set", "gp_iteration",
     "gp_run", "gp_haps_get", "gp_haps_set", "gp_posteriors_get", "gp_states_get", "gp_finalize", "gp_gp_get",
     "gp_impute_batch", "gp_rephase_batch", "gp_select", "gp_pbwt_states_get", "gp_sparse_pbwt_get",
-    "gp_stage_times",
+    "gp_stage_times", "gp_build_sparse_pbwt",
 ]
 
 
@@ -66,6 +66,49 @@ class GpError(RuntimeError):
     pass
 
 
+def _panel_desc(p, keep, ypacked=None, asmall=None):
+    keep.update(cm=np.ascontiguousarray(p.cm, np.float64), cref=np.ascontiguousarray(p.cref, np.uint32),
+                calt=np.ascontiguousarray(p.calt, np.uint32), lq=np.ascontiguousarray(p.lq, np.uint8),
+                common=np.ascontiguousarray(p.flag_common, np.uint8), major=np.ascontiguousarray(p.major, np.uint8),
+                hvar=np.ascontiguousarray(p.hvar, np.uint8), soff=np.ascontiguousarray(p.shap_off, np.int64),
+                ssites=np.ascontiguousarray(p.shap_sites, np.int32))
+    k = keep
+    d = gp_panel_desc()
+    d.n_ref_haps, d.n_sites = p.n_ref_haps, p.n_sites
+    d.cm, d.cref, d.calt = _p(k["cm"], C.c_double), _p(k["cref"], C.c_uint32), _p(k["calt"], C.c_uint32)
+    d.lq, d.flag_common, d.major = _p(k["lq"], C.c_uint8), _p(k["common"], C.c_uint8), _p(k["major"], C.c_uint8)
+    d.hvar, d.shap_off, d.shap_sites = _p(k["hvar"], C.c_uint8), _p(k["soff"], C.c_int64), _p(k["ssites"], C.c_int32)
+    if ypacked is not None:
+        k["yp"] = np.ascontiguousarray(ypacked, np.uint8)
+        d.ypacked, d.ypacked_len = _p(k["yp"], C.c_uint8), k["yp"].size
+    if asmall is not None:
+        k["aoff"] = np.ascontiguousarray(asmall[0], np.int64)
+        k["aidx"] = np.ascontiguousarray(asmall[1], np.int32)
+        d.asmall_off, d.asmall_idx = _p(k["aoff"], C.c_int64), _p(k["aidx"], C.c_int32)
+    return d
+
+
+def build_sparse_pbwt(panel):
+    """Host-only sparse PBWT of a panel: (ypacked, asmall_off, asmall_idx)."""
+    L = lib()
+    keep = {}
+    d = _panel_desc(panel, keep)
+    ylen = C.c_int64(0)
+    alen = C.c_int64(0)
+    rc = L.gp_build_sparse_pbwt(C.byref(d), None, C.byref(ylen), None, None, C.byref(alen))
+    if rc != GP_OK:
+        raise GpError(f"gp_build_sparse_pbwt failed with status {rc}")
+    n_com_hq = int(((panel.flag_common != 0) & (panel.lq == 0)).sum())
+    yp = np.zeros(max(ylen.value, 1), np.uint8)
+    aoff = np.zeros(n_com_hq + 2, np.int64)
+    aidx = np.zeros(max(alen.value, 1), np.int32)
+    rc = L.gp_build_sparse_pbwt(C.byref(d), _p(yp, C.c_uint8), C.byref(ylen), _p(aoff, C.c_int64),
+                                _p(aidx, C.c_int32), C.byref(alen))
+    if rc != GP_OK:
+        raise GpError(f"gp_build_sparse_pbwt failed with status {rc}")
+    return yp[:ylen.value], aoff, aidx[:alen.value]
+
+
 class Context:
     """One device-resident panel plus its targets (a gp_ctx)."""
 
@@ -82,25 +125,8 @@ class Context:
         cfg.seed, cfg.device = seed, device
         self.cfg = cfg
         p = panel
-        self._keep = dict(cm=np.ascontiguousarray(p.cm, np.float64), cref=np.ascontiguousarray(p.cref, np.uint32),
-                          calt=np.ascontiguousarray(p.calt, np.uint32), lq=np.ascontiguousarray(p.lq, np.uint8),
-                          common=np.ascontiguousarray(p.flag_common, np.uint8),
-                          major=np.ascontiguousarray(p.major, np.uint8), hvar=np.ascontiguousarray(p.hvar, np.uint8),
-                          soff=np.ascontiguousarray(p.shap_off, np.int64),
-                          ssites=np.ascontiguousarray(p.shap_sites, np.int32))
-        k = self._keep
-        d = gp_panel_desc()
-        d.n_ref_haps, d.n_sites = p.n_ref_haps, p.n_sites
-        d.cm, d.cref, d.calt = _p(k["cm"], C.c_double), _p(k["cref"], C.c_uint32), _p(k["calt"], C.c_uint32)
-        d.lq, d.flag_common, d.major = _p(k["lq"], C.c_uint8), _p(k["common"], C.c_uint8), _p(k["major"], C.c_uint8)
-        d.hvar, d.shap_off, d.shap_sites = _p(k["hvar"], C.c_uint8), _p(k["soff"], C.c_int64), _p(k["ssites"], C.c_int32)
-        if ypacked is not None:
-            k["yp"] = np.ascontiguousarray(ypacked, np.uint8)
-            d.ypacked, d.ypacked_len = _p(k["yp"], C.c_uint8), k["yp"].size
-        if asmall is not None:
-            k["aoff"] = np.ascontiguousarray(asmall[0], np.int64)
-            k["aidx"] = np.ascontiguousarray(asmall[1], np.int32)
-            d.asmall_off, d.asmall_idx = _p(k["aoff"], C.c_int64), _p(k["aidx"], C.c_int32)
+        self._keep = {}
+        d = _panel_desc(p, self._keep, ypacked, asmall)
         h = C.c_void_p()
         rc = L.gp_ctx_create(C.byref(d), C.byref(cfg), C.byref(h))
         if rc != GP_OK:
@@ -150,3 +176,87 @@ class Context:
                                               _p(h1, C.c_uint8), _p(flat, C.c_uint8), iteration,
                                               _p(ids, C.c_int32)))
         return h0, h1
+
+    # ---- target-level entry points ----
+    def set_targets(self, targets, kpbwt=None):
+        n = targets.n
+        self.n_targets = n
+        self._tk = dict(gl=np.ascontiguousarray(targets.gl, np.uint8), flat=np.ascontiguousarray(targets.flat, np.uint8),
+                        ploidy=np.ascontiguousarray(targets.ploidy, np.int32))
+        kp = None
+        if kpbwt is not None:
+            kp = np.ascontiguousarray(np.broadcast_to(np.asarray(kpbwt, np.int32), (n,)), np.int32)
+            self._tk["kp"] = kp
+        self._check(self.lib.gp_targets_set(self.h, n, _p(self._tk["gl"], C.c_uint8), _p(self._tk["flat"], C.c_uint8),
+                                            _p(self._tk["ploidy"], C.c_int32), _p(kp, C.c_int32)))
+
+    def iteration(self, stage, iteration):
+        self._check(self.lib.gp_iteration(self.h, stage, iteration))
+
+    def select(self, stage, iteration):
+        self._check(self.lib.gp_select(self.h, stage, iteration))
+
+    def run(self, burnin=5, main=15):
+        self._check(self.lib.gp_run(self.h, burnin, main))
+
+    def finalize(self):
+        self._check(self.lib.gp_finalize(self.h))
+
+    def haps(self):
+        h0 = np.zeros((self.n_targets, self.L), np.uint8)
+        h1 = np.zeros((self.n_targets, self.L), np.uint8)
+        self._check(self.lib.gp_haps_get(self.h, _p(h0, C.c_uint8), _p(h1, C.c_uint8)))
+        return h0, h1
+
+    def set_haps(self, h0, h1):
+        h0 = np.ascontiguousarray(h0, np.uint8)
+        h1 = np.ascontiguousarray(h1, np.uint8)
+        self._check(self.lib.gp_haps_set(self.h, _p(h0, C.c_uint8), _p(h1, C.c_uint8)))
+
+    def posteriors(self, target):
+        hp0 = np.zeros(2 * self.L, np.float32)
+        hp1 = np.zeros(2 * self.L, np.float32)
+        self._check(self.lib.gp_posteriors_get(self.h, target, _p(hp0, C.c_float), _p(hp1, C.c_float)))
+        return hp0, hp1
+
+    def states(self, target):
+        out = np.zeros(self.N, np.uint32)
+        n = C.c_int32(0)
+        self._check(self.lib.gp_states_get(self.h, target, _p(out, C.c_uint32), C.byref(n)))
+        return out[:n.value].copy()
+
+    def pbwt_states(self, target, depth=None):
+        depth = depth or self.cfg.pbwt_depth
+        counts = np.zeros(depth, np.int32)
+        buf = np.zeros(1 << 22, np.int32)
+        self._check(self.lib.gp_pbwt_states_get(self.h, target, _p(counts, C.c_int32), _p(buf, C.c_int32), buf.size))
+        out, o = [], 0
+        for c in counts:
+            out.append(buf[o:o + c].copy())
+            o += c
+        return out
+
+    def gp(self):
+        shape = (self.n_targets, self.L)
+        gp0, gp1, ds = (np.zeros(shape, np.float32) for _ in range(3))
+        gt0, gt1 = np.zeros(shape, np.uint8), np.zeros(shape, np.uint8)
+        self._check(self.lib.gp_gp_get(self.h, _p(gp0, C.c_float), _p(gp1, C.c_float), _p(ds, C.c_float),
+                                       _p(gt0, C.c_uint8), _p(gt1, C.c_uint8)))
+        return gp0, gp1, ds, gt0, gt1
+
+    def stage_times(self):
+        ms = np.zeros(5, np.float32)
+        self._check(self.lib.gp_stage_times(self.h, _p(ms, C.c_float), 5))
+        return ms
+
+    def sparse_pbwt(self):
+        ylen = C.c_int64(0)
+        alen = C.c_int64(0)
+        self._check(self.lib.gp_sparse_pbwt_get(self.h, None, C.byref(ylen), None, None, C.byref(alen)))
+        n_com_hq = int(((self.panel.flag_common != 0) & (self.panel.lq == 0)).sum())
+        yp = np.zeros(max(ylen.value, 1), np.uint8)
+        aoff = np.zeros(n_com_hq + 2, np.int64)
+        aidx = np.zeros(max(alen.value, 1), np.int32)
+        self._check(self.lib.gp_sparse_pbwt_get(self.h, _p(yp, C.c_uint8), C.byref(ylen), _p(aoff, C.c_int64),
+                                                _p(aidx, C.c_int32), C.byref(alen)))
+        return yp[:ylen.value], aoff, aidx[:alen.value]

@@ -153,6 +153,13 @@ int gp_pbwt_states_get(gp_ctx* ctx, int32_t target, int32_t* counts, int32_t* st
 int gp_sparse_pbwt_get(gp_ctx* ctx, uint8_t* ypacked, int64_t* ypacked_len, int64_t* asmall_off,
                        int32_t* asmall_idx, int64_t* asmall_len);
 
+/* The same sparse PBWT built from a panel descriptor on the host, without a
+ * context or a GPU (offline panel preparation, as GLIMPSE2_split_reference
+ * does through ref_haplotype_set::build_sparsePBWT). Call once with NULL
+ * buffers to get the lengths; asmall_off has n_common_hq + 2 entries. */
+int gp_build_sparse_pbwt(const gp_panel_desc* panel, uint8_t* ypacked, int64_t* ypacked_len, int64_t* asmall_off,
+                         int32_t* asmall_idx, int64_t* asmall_len);
+
 /* Timing of the last gp_iteration by stage, in milliseconds (device events). */
 int gp_stage_times(gp_ctx* ctx, float* ms, int32_t n);
 

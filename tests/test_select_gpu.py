@@ -1,0 +1,61 @@
+"""State selection parity (bit-exact):
+  * init stage: haplotype_set::initRareTar + performSelection_RARE_INIT_GL
+    (haplotype_set.cpp:108-169,775-833), per-target std::sample streams;
+  * burn-in/main: matchHapsFromCompressedPBWTSmall (haplotype_set.cpp:317-394),
+    every pbwt_states level list, and the conditioning_set::compactSelection
+    union (conditioning_set.cpp:96-104)."""
+import numpy as np
+import pytest
+
+from conftest import ref_oracle_or_skip
+
+
+def _noisy(rng, h, p):
+    h = h.copy()
+    h[rng.random(h.shape) < p] ^= 1
+    return h
+
+
+@pytest.fixture(scope="module")
+def pair(small_workload):
+    O = ref_oracle_or_skip()
+    from glimpse_b200 import native
+    w = small_workload
+    kw = dict(kinit=200, kpbwt=int(w.targets.kpbwt.max()), pbwt_depth=8, pbwt_modulo_cm=0.05)
+    orc = O.RefOracle(w.panel, w.targets, kpbwt_target=w.targets.kpbwt, **kw)
+    ctx = native.Context(w.panel, **kw)
+    ctx.set_targets(w.targets, kpbwt=w.targets.kpbwt)
+    return w, orc, ctx, O
+
+
+@pytest.mark.gpu
+def test_init_selection_matches_reference(pair):
+    w, orc, ctx, O = pair
+    orc.init_select(0)
+    ctx.select(O.STAGE_INIT, 0)
+    for t in range(w.targets.n):
+        ref = np.sort(orc.init_states(t)).astype(np.uint32)
+        got = ctx.states(t)
+        assert np.array_equal(ref, got), f"target {t}: {len(ref)} vs {len(got)} states"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("it,noise", [(1, 0.0), (4, 0.02), (9, 0.1)])
+def test_pbwt_selection_matches_reference(pair, it, noise):
+    w, orc, ctx, O = pair
+    rng = np.random.default_rng(it)
+    T = w.targets
+    h0 = np.stack([_noisy(rng, T.truth[t, 0], noise) for t in range(T.n)])
+    h1 = np.stack([_noisy(rng, T.truth[t, 1], noise) for t in range(T.n)])
+    for t in range(T.n):
+        orc.set_haps(t, h0[t], h1[t])
+    ctx.set_haps(h0, h1)
+    orc.pbwt_select(it, main_iteration=False)
+    ctx.select(O.STAGE_BURN, it)
+    for t in range(T.n):
+        ref_lv = orc.pbwt_states(t)
+        got_lv = ctx.pbwt_states(t, depth=len(ref_lv))
+        for lv, (r, g) in enumerate(zip(ref_lv, got_lv)):
+            assert np.array_equal(r, g), f"target {t} level {lv}: {r[:10]} vs {g[:10]} ({len(r)} vs {len(g)})"
+        ref_states = orc.select(t, O.STAGE_BURN)
+        assert np.array_equal(ref_states, ctx.states(t)), f"target {t} union differs"
