@@ -14,7 +14,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 # --fmad=false: the kernels place every fused multiply-add explicitly (fmaf) where
 # the reference's compiled arithmetic has one, so no other contraction may happen.
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "--fmad=false", "-std=c++17",
-              "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "-shared", "-ccbin", "/usr/bin/g++"]
+              "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "-Xcompiler", "-g", "-shared", "-ccbin", "/usr/bin/g++"]
 
 
 def sources():

@@ -46,6 +46,42 @@ ModelConst model_constants(const gp_config& c, int n_ref_haps) {
   return m;
 }
 
+void Context::prof_begin(cudaEvent_t& a) {
+  cudaEventCreate(&a);
+  cudaEventRecord(a, stream);
+}
+
+void Context::prof_end(cudaEvent_t a, int kind, double cells) {
+  cudaEvent_t b;
+  cudaEventCreate(&b);
+  cudaEventRecord(b, stream);
+  prof_pending.push_back({a, b, kind, cells});
+}
+
+// Called after a stream synchronisation: accumulates the event pairs.
+void Context::prof_resolve() {
+  for (auto& p : prof_pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+      if (p.kind == 0) {
+        prof.impute_ms += ms;
+        prof.impute_cells += p.cells;
+        prof.impute_bytes += p.cells * 8.25;  // 1/8 B Hvar + 4 B alpha, forward and backward
+        prof.impute_launches++;
+      } else if (p.kind == 1) {
+        prof.phase_ms += ms;
+        prof.phase_cells += p.cells;
+        prof.phase_launches++;
+      } else {
+        prof.select_ms += ms;
+      }
+    }
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+  }
+  prof_pending.clear();
+}
+
 Status Context::fail(int code, const std::string& msg) {
   err = msg;
   Status s;
@@ -154,6 +190,12 @@ int Context::create_panel(const gp_panel_desc& d) {
   } else {
     cudaMemsetAsync(P.refT, 0, sizeof(uint32_t) * N * P.W, stream);
   }
+  {
+    std::string msg;
+    if (validate_panel(N, L, host.lq.data(), host.common.data(), host.major.data(), host.cref.data(),
+                       host.calt.data(), host.hvar.data(), host.svar_off.data(), msg) != GP_OK)
+      return (fail(GP_E_DATA, "panel: " + msg), GP_E_DATA);
+  }
   // Sparse PBWT: supplied with the panel (binary panel format) or built here.
   if (d.ypacked && d.asmall_off && d.asmall_idx) {
     sparse.ypacked.assign(d.ypacked, d.ypacked + d.ypacked_len);
@@ -178,6 +220,7 @@ Context::~Context() {
   impute.hvar.release(); impute.em.release(); impute.tr.release(); impute.fl.release();
   impute.alpha.release(); impute.alpha_off.release();
   impute.hl.release(); impute.hp.release(); impute.flat.release();
+  prof_resolve();
   for (DevBuf* b : phase.all()) b->release();
   for (DevBuf* b : tw.all()) b->release();
   scratch_h0.release(); scratch_h1.release(); scratch_ids.release();
@@ -225,6 +268,7 @@ int Context::build_condsets(int n, const std::vector<int64_t>& off, const std::v
   launch_mark_poly(panel, w, stream);
   launch_compact_poly(panel, w, stream);
   launch_build_hvar(panel, w, stream);
+  prof.kernel_launches += 5;
   impute_np.assign(n, 0);
   cudaMemcpyAsync(impute_np.data(), w.npoly.ptr, n * 4, cudaMemcpyDeviceToHost, stream);
   if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(e, "conditioning set");
@@ -249,8 +293,14 @@ int Context::run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
   if ((e = w.alpha.ensure((size_t)std::max<int64_t>(tot, 1) * 4)) != cudaSuccess) return cuda_fail(e, "alloc alpha");
   cudaMemcpyAsync(w.alpha_off.ptr, aoff.data(), n * 8, cudaMemcpyHostToDevice, stream);
   launch_site_records(panel, mc, w, d_hl, d_flat, stream);
+  double cells = 0;
+  for (int i = 0; i < n; ++i) cells += (double)impute_np[i] * (double)host_nstates[i];
+  cudaEvent_t ea;
+  prof_begin(ea);
   launch_impute_fb(mc, w, d_hp, stream);
+  prof_end(ea, 0, cells);
   launch_impute_mono(panel, mc, w, d_hl, d_flat, d_hp, stream);
+  prof.kernel_launches += 3;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "imputation launch");
   return GP_OK;
 }
@@ -280,6 +330,7 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   V.nmiss = V.nvar + 2 * nb;
   launch_build_vars(d_tsel, nb, w.poly.as<int32_t>(), w.npoly.as<int32_t>(), d_h0, d_h1, d_flat, panel.lq, L, V,
                     stream);
+  prof.kernel_launches += 1;
   std::vector<int32_t> cnt((size_t)nb * 3);
   cudaMemcpyAsync(cnt.data(), p.counts.ptr, cnt.size() * 4, cudaMemcpyDeviceToHost, stream);
   if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(e, "phasing vars");
@@ -319,11 +370,20 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   S.dip = p.dip.as<int32_t>();
   S.err = p.err.as<int32_t>();
   const int J = std::max(1, (Kmax + kPhaseThreads - 1) / kPhaseThreads);
+  double pcells = 0;
+  for (int b = 0; b < nb; ++b) {
+    const int t = tsel_host.empty() ? b : tsel_host[b];
+    pcells += 2.0 * 8.0 * (double)cnt[b] * (double)host_nstates[t];
+  }
+  cudaEvent_t ea;
+  prof_begin(ea);
   if (launch_phase(J, d_tsel, nb, w.nstates.as<int32_t>(), w.hvar.as<uint32_t>(), w.WB, w.Kp, w.poly.as<int32_t>(),
                    L, panel.cm, V, S, mc, cfg.seed, iteration, d_target_ids, stream) != GP_OK)
     return (fail(GP_E_ARG, "phasing: too many states"), GP_E_ARG);
+  prof_end(ea, 1, pcells);
   launch_phase_writeback(d_tsel, nb, w.poly.as<int32_t>(), w.polyidx.as<int32_t>(), L, V, S, mc, cfg.seed, iteration,
                          d_target_ids, d_h0, d_h1, stream);
+  prof.kernel_launches += 3;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "phasing launch");
   last_phase_nseg.assign(cnt.begin() + nb, cnt.begin() + 2 * nb);
   return GP_OK;
@@ -399,6 +459,7 @@ int gp_impute_batch(gp_ctx* ctx, int32_t n, const int64_t* states_off, const uin
   if (rc != GP_OK) return rc;
   cudaMemcpyAsync(hp, w.hp.ptr, (size_t)n * 2 * L * 4, cudaMemcpyDeviceToHost, c.stream);
   if ((e = cudaStreamSynchronize(c.stream)) != cudaSuccess) return c.cuda_fail(e, "impute");
+  c.prof_resolve();
   return GP_OK;
 }
 
@@ -433,6 +494,7 @@ int gp_rephase_batch(gp_ctx* ctx, int32_t n, const int64_t* states_off, const ui
   cudaMemcpyAsync(h0, bh0.ptr, (size_t)n * L, cudaMemcpyDeviceToHost, c.stream);
   cudaMemcpyAsync(h1, bh1.ptr, (size_t)n * L, cudaMemcpyDeviceToHost, c.stream);
   if ((e = cudaStreamSynchronize(c.stream)) != cudaSuccess) return c.cuda_fail(e, "rephase");
+  c.prof_resolve();
   return GP_OK;
 }
 

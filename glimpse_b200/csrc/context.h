@@ -69,6 +69,17 @@ struct Context {
   std::vector<int32_t> pbwt_grp;
   int tw_push_cap = 4096;
   float stage_ms[5] = {0, 0, 0, 0, 0};
+  // profiling: events around the hot kernels, resolved at the next host sync
+  struct ProfEv {
+    cudaEvent_t a, b;
+    int kind;  // 0 imputation forward-backward, 1 phasing, 2 selection
+    double cells;
+  };
+  std::vector<ProfEv> prof_pending;
+  gp_profile prof{};
+  void prof_begin(cudaEvent_t& a);
+  void prof_end(cudaEvent_t a, int kind, double cells);
+  void prof_resolve();
   std::vector<void*> owned;  // device allocations freed at destruction
 
   ~Context();

@@ -153,6 +153,7 @@ int Context::select_states(int stage, int iteration, int& Kp) {
     a.seed = cfg.seed;
     a.iteration = iteration;
     launch_init_select(a, stream);
+    prof.kernel_launches += 2;
     return GP_OK;
   }
   return pbwt_select_states(stage, iteration, Kp);
@@ -175,19 +176,23 @@ int Context::iteration(int stage, int iteration) {
   // first haplotype (caller_algorithm.cpp:58-65)
   launch_hl(T.gl.as<uint8_t>(), T.flat.as<uint8_t>(), T.ploidy.as<int32_t>(), T.h0.as<uint8_t>(),
             T.h1.as<uint8_t>(), n, L, stage == GP_STAGE_INIT, 0, mc.min_gl, T.hl.as<float>(), stream);
+  prof.kernel_launches += 1;
   rc = run_impute(T.hl.as<float>(), T.flat.as<uint8_t>(), T.hp0.as<float>());
   if (rc != GP_OK) return rc;
   launch_sample(T.hp0.as<float>(), T.ploidy.as<int32_t>(), n, L, cfg.seed, RNG_SAMPLE_H0, iteration, 0,
                 T.h0.as<uint8_t>(), stream);
+  prof.kernel_launches += 1;
   cudaEventRecord(ev[2], stream);
   if (!T.diploid.empty()) {
     // second haplotype and phasing (caller_algorithm.cpp:66-72)
     launch_hl(T.gl.as<uint8_t>(), T.flat.as<uint8_t>(), T.ploidy.as<int32_t>(), T.h0.as<uint8_t>(),
               T.h1.as<uint8_t>(), n, L, 0, 1, mc.min_gl, T.hl.as<float>(), stream);
+    prof.kernel_launches += 1;
     rc = run_impute(T.hl.as<float>(), T.flat.as<uint8_t>(), T.hp1.as<float>());
     if (rc != GP_OK) return rc;
     launch_sample(T.hp1.as<float>(), T.ploidy.as<int32_t>(), n, L, cfg.seed, RNG_SAMPLE_H1, iteration, 1,
                   T.h1.as<uint8_t>(), stream);
+    prof.kernel_launches += 1;
     cudaEventRecord(ev[3], stream);
     const bool all = (int)T.diploid.size() == n;
     rc = run_phase(all ? nullptr : T.dip_list.as<int32_t>(), all ? std::vector<int32_t>() : T.diploid,
@@ -201,6 +206,7 @@ int Context::iteration(int stage, int iteration) {
   if (stage == GP_STAGE_MAIN) {
     launch_gp_store(T.hp0.as<float>(), T.hp1.as<float>(), T.ploidy.as<int32_t>(), n, L, T.stored_cnt,
                     T.gp0.as<float>(), T.gp1.as<float>(), T.gpflags.as<uint8_t>(), stream);
+    prof.kernel_launches += 1;
     T.stored_cnt++;
   }
   cudaEventRecord(ev[5], stream);
@@ -209,6 +215,8 @@ int Context::iteration(int stage, int iteration) {
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "iteration launch");
   for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&stage_ms[i], ev[i], ev[i + 1]);
   for (auto& x : ev) cudaEventDestroy(x);
+  prof.select_ms += stage_ms[0];
+  prof_resolve();
   return GP_OK;
 }
 
@@ -219,6 +227,7 @@ int Context::finalize() {
   launch_gp_finalize(T.ploidy.as<int32_t>(), T.n, panel.L, T.stored_cnt, T.gpflags.as<uint8_t>(), T.gp0.as<float>(),
                      T.gp1.as<float>(), T.ds.as<float>(), T.gt0.as<uint8_t>(), T.gt1.as<uint8_t>(),
                      T.h0.as<uint8_t>(), T.h1.as<uint8_t>(), stream);
+  prof.kernel_launches += 1;
   cudaError_t e = cudaStreamSynchronize(stream);
   if (e != cudaSuccess) return cuda_fail(e, "finalize");
   T.finalized = true;
@@ -334,6 +343,42 @@ int gp_gp_get(gp_ctx* ctx, float* gp0, float* gp1, float* ds, uint8_t* gt0, uint
   cudaError_t e = cudaStreamSynchronize(c.stream);
   return e == cudaSuccess ? GP_OK : c.cuda_fail(e, "gp_get");
 }
+
+int gp_targets_reset(gp_ctx* ctx) {
+  if (!ctx) return GP_E_ARG;
+  Context& c = *C_(ctx);
+  gp::TargetWork& T = c.tw;
+  if (T.n <= 0) return (c.fail(GP_E_STATE, "no targets"), GP_E_STATE);
+  const size_t nL = (size_t)T.n * c.panel.L;
+  cudaMemsetAsync(T.h0.ptr, 0, nL, c.stream);
+  cudaMemsetAsync(T.h1.ptr, 0, nL, c.stream);
+  cudaMemsetAsync(T.gpflags.ptr, 0, nL, c.stream);
+  cudaMemsetAsync(T.gp0.ptr, 0, nL * 4, c.stream);
+  cudaMemsetAsync(T.gp1.ptr, 0, nL * 4, c.stream);
+  cudaMemsetAsync(T.tar_hap.ptr, 0, T.hap_target.size(), c.stream);
+  T.stored_cnt = 0;
+  T.finalized = false;
+  cudaError_t e = cudaStreamSynchronize(c.stream);
+  return e == cudaSuccess ? GP_OK : c.cuda_fail(e, "targets_reset");
+}
+
+int gp_profile_get(gp_ctx* ctx, gp_profile* out) {
+  if (!ctx || !out) return GP_E_ARG;
+  Context& c = *C_(ctx);
+  c.prof_resolve();
+  *out = c.prof;
+  return GP_OK;
+}
+
+int gp_profile_reset(gp_ctx* ctx) {
+  if (!ctx) return GP_E_ARG;
+  Context& c = *C_(ctx);
+  c.prof_resolve();
+  c.prof = gp_profile{};
+  return GP_OK;
+}
+
+void* gp_stream(gp_ctx* ctx) { return ctx ? (void*)C_(ctx)->stream : nullptr; }
 
 int gp_stage_times(gp_ctx* ctx, float* ms, int32_t n) {
   if (!ctx || !ms) return GP_E_ARG;

@@ -65,6 +65,40 @@ void column_update(std::vector<uint32_t>& a, std::vector<uint32_t>& b, int zeros
 
 }  // namespace
 
+int validate_panel(int N, int L, const uint8_t* lq, const uint8_t* common, const uint8_t* major,
+                   const uint32_t* cref, const uint32_t* calt, const uint8_t* hvar, const int64_t* svar_off,
+                   std::string& msg) {
+  (void)lq;
+  const size_t stride = ((size_t)N + 7) / 8;
+  int row = 0;
+  for (int k = 0; k < L; ++k) {
+    if ((int64_t)cref[k] + (int64_t)calt[k] != N) {
+      msg = "site " + std::to_string(k) + ": cref + calt differs from the number of reference haplotypes";
+      return GP_E_DATA;
+    }
+    if (common[k]) {
+      int64_t ones = 0;
+      const uint8_t* r = hvar + (size_t)row * stride;
+      for (size_t b = 0; b < stride; ++b) ones += __builtin_popcount(r[b]);
+      if (ones != (int64_t)calt[k]) {
+        msg = "common site " + std::to_string(k) + ": HvarRef row has " + std::to_string(ones) +
+              " alternative alleles, calt says " + std::to_string(calt[k]);
+        return GP_E_DATA;
+      }
+      ++row;
+    } else {
+      const int64_t nc = svar_off[k + 1] - svar_off[k];
+      const int64_t want = major[k] ? cref[k] : calt[k];
+      if (nc != want) {
+        msg = "rare site " + std::to_string(k) + ": ShapRef lists " + std::to_string(nc) +
+              " carriers of the non-major allele, the counts say " + std::to_string(want);
+        return GP_E_DATA;
+      }
+    }
+  }
+  return GP_OK;
+}
+
 void build_sparse_pbwt(int N, int L, const uint8_t* lq, const uint8_t* common, const uint8_t* major,
                        const uint32_t* cref, const uint32_t* calt, const uint8_t* hvar, const int64_t* svar_off,
                        const int32_t* svar_haps, SparsePbwt& out) {
@@ -217,6 +251,7 @@ int Context::pbwt_prepare_panel() {
   // and its rank bits; returns false on a malformed stream.
   auto decode = [&](std::vector<uint32_t>& a, std::vector<uint32_t>& b, int n, int zeros, uint32_t* bits,
                     uint32_t* pref, int W) -> bool {
+    if (zeros < 0 || zeros > n) return false;
     int u = 0, v = zeros, m = 0;
     std::fill(bits, bits + W, 0u);
     while (m < n) {
@@ -226,6 +261,7 @@ int Context::pbwt_prepare_panel() {
       const int sym = z >> 7;
       if (len <= 0 || m + len > n) return false;
       int& occ = sym ? v : u;
+      if (occ + len > (sym ? n : zeros)) return false;  // column counts disagree with cref/calt
       for (int i = m; i < m + len; ++i) {
         b[occ++] = a[i];
         if (sym) bits[i >> 5] |= 1u << (i & 31);
@@ -446,6 +482,7 @@ int Context::pbwt_select_states(int stage, int iteration, int Kp) {
   a.iteration = iteration;
   cudaMemsetAsync(T.overflow.ptr, 0, 4, stream);
   launch_pbwt_select(a, stream);
+  prof.kernel_launches += 3;
   int32_t ovf = 0;
   cudaMemcpyAsync(&ovf, T.overflow.ptr, 4, cudaMemcpyDeviceToHost, stream);
   cudaError_t e = cudaStreamSynchronize(stream);
@@ -522,6 +559,9 @@ int gp_build_sparse_pbwt(const gp_panel_desc* d, uint8_t* ypacked, int64_t* ypac
   std::vector<int64_t> fill(so.begin(), so.end() - 1);
   for (int h = 0; h < N; ++h)
     for (int64_t j = d->shap_off[h]; j < d->shap_off[h + 1]; ++j) sh[fill[d->shap_sites[j]]++] = h;
+  std::string msg;
+  if (gp::validate_panel(N, L, d->lq, d->flag_common, d->major, d->cref, d->calt, d->hvar, so.data(), msg) != GP_OK)
+    return GP_E_DATA;
   gp::SparsePbwt sp;
   gp::build_sparse_pbwt(N, L, d->lq, d->flag_common, d->major, d->cref, d->calt, d->hvar, so.data(), sh.data(), sp);
   if (ypacked_len) *ypacked_len = (int64_t)sp.ypacked.size();

@@ -1,6 +1,7 @@
 // PBWT state selection: panel-side precompute (pbwt_host.cpp) and the
 // per-iteration device kernels (kernels_pbwt.cu).
 #pragma once
+#include <string>
 #include <vector>
 
 #include "internal.h"
@@ -16,6 +17,13 @@ struct SparsePbwt {
   std::vector<int64_t> asmall_off;  // [n_com_hq + 2]
   std::vector<int32_t> asmall;      // positions in the full PBWT order, sorted
 };
+
+// Consistency of the panel arrays the PBWT relies on: cref + calt = N, the
+// HvarRef row of every common site has calt ones, and every rare site lists as
+// many non-major carriers as its counts say. Returns GP_OK or GP_E_DATA (msg set).
+int validate_panel(int N, int L, const uint8_t* lq, const uint8_t* common, const uint8_t* major,
+                   const uint32_t* cref, const uint32_t* calt, const uint8_t* hvar, const int64_t* svar_off,
+                   std::string& msg);
 
 // ref_haplotype_set::build_sparsePBWT (ref_haplotype_set.cpp:47-193) over the
 // in-memory panel, restated: pack3 run-length coding of every HQ common column in

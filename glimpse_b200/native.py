@@ -21,8 +21,17 @@ EXPORTS = [
     "gp_config_defaults", "gp_ctx_create", "gp_ctx_destroy", "gp_last_error", "gp_targets_set", "gp_iteration",
     "gp_run", "gp_haps_get", "gp_haps_set", "gp_posteriors_get", "gp_states_get", "gp_finalize", "gp_gp_get",
     "gp_impute_batch", "gp_rephase_batch", "gp_select", "gp_pbwt_states_get", "gp_sparse_pbwt_get",
-    "gp_stage_times", "gp_build_sparse_pbwt",
+    "gp_stage_times", "gp_build_sparse_pbwt", "gp_profile_get", "gp_profile_reset", "gp_stream",
+    "gp_targets_reset",
 ]
+
+
+class gp_profile(C.Structure):
+    _fields_ = [
+        ("impute_ms", C.c_double), ("impute_cells", C.c_double), ("impute_bytes", C.c_double),
+        ("phase_ms", C.c_double), ("phase_cells", C.c_double), ("select_ms", C.c_double),
+        ("impute_launches", C.c_int64), ("phase_launches", C.c_int64), ("kernel_launches", C.c_int64),
+    ]
 
 
 class gp_panel_desc(C.Structure):
@@ -55,6 +64,8 @@ def lib():
         _lib = C.CDLL(LIB_PATH)
         _lib.gp_last_error.restype = C.c_char_p
         _lib.gp_last_error.argtypes = [C.c_void_p]
+        _lib.gp_stream.restype = C.c_void_p
+        _lib.gp_stream.argtypes = [C.c_void_p]
     return _lib
 
 
@@ -260,3 +271,28 @@ class Context:
         self._check(self.lib.gp_sparse_pbwt_get(self.h, _p(yp, C.c_uint8), C.byref(ylen), _p(aoff, C.c_int64),
                                                 _p(aidx, C.c_int32), C.byref(alen)))
         return yp[:ylen.value], aoff, aidx[:alen.value]
+
+    def targets_reset(self):
+        self._check(self.lib.gp_targets_reset(self.h))
+
+    def profile(self):
+        p = gp_profile()
+        self._check(self.lib.gp_profile_get(self.h, C.byref(p)))
+        return {f: getattr(p, f) for f, _ in gp_profile._fields_}
+
+    def profile_reset(self):
+        self._check(self.lib.gp_profile_reset(self.h))
+
+    def stream_handle(self) -> int:
+        return int(self.lib.gp_stream(self.h) or 0)
+
+    def set_targets_raw(self, n, gl_ptr, flat_ptr, ploidy_ptr, kpbwt_ptr):
+        """gp_targets_set from raw host pointers (e.g. pinned buffers)."""
+        self.n_targets = n
+        self._check(self.lib.gp_targets_set(self.h, n, C.c_void_p(gl_ptr), C.c_void_p(flat_ptr),
+                                            C.c_void_p(ploidy_ptr), C.c_void_p(kpbwt_ptr)))
+
+    def gp_raw(self, ds_ptr, gt0_ptr, gt1_ptr):
+        """gp_gp_get of the dosages and called alleles into raw host pointers."""
+        self._check(self.lib.gp_gp_get(self.h, None, None, C.c_void_p(ds_ptr), C.c_void_p(gt0_ptr),
+                                       C.c_void_p(gt1_ptr)))

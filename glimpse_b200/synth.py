@@ -132,69 +132,82 @@ def make_panel_and_targets(n_ref_haps, n_sites, region_mb, rare_frac, n_targets,
     com_cm = cm[com_idx]
 
     def founder_path(n_h):
-        """Founder index per (hap, common site), uint8 [n_h, n_common]."""
-        path = np.empty((n_h, n_common), dtype=np.uint8)
+        """Founder index per (hap, common site), uint8 [n_h, n_common]: Poisson
+        switch points per haplotype, a fresh founder after each switch."""
         n_sw = rng.poisson(switches_per_cm * length_cm, n_h)
-        for h in range(n_h):
-            pts = np.sort(rng.uniform(0.0, length_cm, n_sw[h]))
-            seg = np.searchsorted(pts, com_cm, side="right")
-            fids = rng.integers(0, n_founders, n_sw[h] + 1).astype(np.uint8)
-            path[h] = fids[seg]
-        return path
+        tot = int(n_sw.sum())
+        hap_of = np.repeat(np.arange(n_h), n_sw)
+        sw_site = np.searchsorted(com_cm, rng.uniform(0.0, length_cm, tot), side="right")
+        delta = np.zeros((n_h, n_common + 1), dtype=np.int16)
+        np.add.at(delta, (hap_of, sw_site), 1)
+        seg = np.cumsum(delta[:, :n_common], axis=1, dtype=np.int16)
+        fids = rng.integers(0, n_founders, (n_h, int(n_sw.max()) + 1 if n_h else 1)).astype(np.uint8)
+        return np.take_along_axis(fids, seg.astype(np.int64), axis=1)
 
     # Haplotypes processed in chunks of 8 so bits pack straight into HvarRef.
     stride = (N + 7) // 8
     hvar_all = np.zeros((n_common, (n_all + 7) // 8), dtype=np.uint8)
     tar_common = np.zeros((n_tar_haps, n_common), dtype=np.uint8)
-    # founder ids at a few rare-site anchors, for clustering rare carriers
     rare_idx = np.flatnonzero(is_rare)
-    rare_anchor = np.searchsorted(com_idx, rare_idx).clip(0, max(n_common - 1, 0))
-    rare_founder = np.zeros((n_all, rare_idx.size), dtype=np.uint8) if rare_idx.size else None
+    path_all = np.zeros((n_all, n_common), dtype=np.uint8) if rare_idx.size else None
     chunk = 2048
     for h0 in range(0, n_all, chunk):
         h1 = min(n_all, h0 + chunk)
         path = founder_path(h1 - h0)
         bits = F[path, np.arange(n_common)[None, :]]
-        mut = rng.random(bits.shape) < mutation
-        bits ^= mut.astype(np.uint8)
-        if rare_founder is not None and n_common:
-            rare_founder[h0:h1] = path[:, rare_anchor]
-        # place haps: panel first, then targets
-        for hh in range(h0, h1):
-            if hh >= N:
-                tar_common[hh - N] = bits[hh - h0]
+        bits ^= (rng.random(bits.shape, dtype=np.float32) < mutation).astype(np.uint8)
+        if path_all is not None:
+            path_all[h0:h1] = path
+        if h1 > N:
+            lo = max(h0, N)
+            tar_common[lo - N:h1 - N] = bits[lo - h0:h1 - h0]
         packed = np.packbits(bits.T, axis=1)  # [n_common, ceil((h1-h0)/8)]
-        if h0 % 8 == 0:
-            hvar_all[:, h0 // 8: h0 // 8 + packed.shape[1]] |= packed
-        else:  # not reached (chunk is a multiple of 8)
-            raise AssertionError
+        hvar_all[:, h0 // 8: h0 // 8 + packed.shape[1]] |= packed
     # panel-only HvarRef: clear padding bits beyond N in the last byte
     hvar = np.ascontiguousarray(hvar_all[:, :stride])
     if N % 8:
         hvar[:, -1] &= np.uint8((0xFF << (8 - N % 8)) & 0xFF)
 
-    # Rare alleles: MAC from 1/x on [1, ceil(sparse_maf*N)-1], carriers drawn
-    # among haps that copy the same founder at the nearest common site.
+    # Rare alleles: MAC from 1/x on [1, ceil(sparse_maf*N)-1]; carriers are
+    # haplotypes that copy the origin's founder at the nearest common site,
+    # found among random probes of the population.
     max_mac = max(1, int(math.ceil(sparse_maf * N)) - 1)
     rare_carriers = []
     tar_rare_carriers = []
     if rare_idx.size:
-        macs = np.floor(np.exp(rng.uniform(0.0, math.log(max_mac + 1), rare_idx.size))).astype(np.int64)
+        nr = rare_idx.size
+        anchor = np.searchsorted(com_idx, rare_idx).clip(0, max(n_common - 1, 0))
+        macs = np.floor(np.exp(rng.uniform(0.0, math.log(max_mac + 1), nr))).astype(np.int64)
         macs = np.clip(macs, 1, max_mac)
-        origin = rng.integers(0, n_all, rare_idx.size)
-        for j in range(rare_idx.size):
-            fid = rare_founder[origin[j], j]
-            pool = np.flatnonzero(rare_founder[:, j] == fid)
-            pool_ref = pool[pool < N]
-            pool_tar = pool[pool >= N] - N
-            if pool_ref.size == 0:
-                pool_ref = np.arange(N)
-            mac = min(int(macs[j]), pool_ref.size)
-            ref_car = np.sort(rng.choice(pool_ref, size=mac, replace=False))
-            p_tar = mac / pool_ref.size
-            tar_car = pool_tar[rng.random(pool_tar.size) < p_tar]
-            rare_carriers.append(ref_car)
-            tar_rare_carriers.append(np.sort(tar_car))
+        origin = rng.integers(0, N, nr)
+        fo = path_all[origin, anchor]
+        P = 64 * n_founders // 10 + 64
+        probes = rng.integers(0, n_all, (nr, P))
+        match = path_all[probes, anchor[:, None]] == fo[:, None]
+        probes_ref = np.where(match & (probes < N), probes, -1)
+        probes_tar = np.where(match & (probes >= N), probes - N, -1)
+        # the origin always carries; other carriers are distinct matching probes in random order
+        cand = np.concatenate([origin[:, None], probes_ref], axis=1)
+        cand = np.sort(cand, axis=1)
+        dup = np.zeros_like(cand, dtype=bool)
+        dup[:, 1:] = cand[:, 1:] == cand[:, :-1]
+        valid = (cand >= 0) & ~dup
+        key = rng.random(cand.shape, dtype=np.float32)
+        key[~valid] = 2.0
+        key[(cand == origin[:, None]) & valid] = -1.0
+        order = np.argsort(key, axis=1)
+        cand = np.take_along_axis(cand, order, axis=1)
+        valid = np.take_along_axis(valid, order, axis=1)
+        take = valid & (np.arange(cand.shape[1])[None, :] < macs[:, None])
+        tcand = np.sort(probes_tar, axis=1)
+        tdup = np.zeros_like(tcand, dtype=bool)
+        tdup[:, 1:] = tcand[:, 1:] == tcand[:, :-1]
+        tkeep = (tcand >= 0) & ~tdup & (rng.random(tcand.shape, dtype=np.float32) <
+                                         (macs / max(1.0, N / n_founders))[:, None])
+        for j in range(nr):
+            rare_carriers.append(np.sort(cand[j, take[j]]))
+            tar_rare_carriers.append(tcand[j, tkeep[j]])
+        del path_all, probes, match
 
     # Site counts and classes.
     calt = np.zeros(L, dtype=np.int64)
@@ -205,16 +218,17 @@ def make_panel_and_targets(n_ref_haps, n_sites, region_mb, rare_frac, n_targets,
     for j, s in enumerate(rare_idx):
         calt[s] = rare_carriers[j].size
     cref = N - calt
-    # keep every site polymorphic in the panel (reference drops monomorphic sites)
-    mono = (calt == 0) | (cref == 0)
-    if mono.any():
-        for s in np.flatnonzero(mono):
-            ci = np.searchsorted(com_idx, s)
-            h = int(rng.integers(0, N))
-            byte, bit = h // 8, 7 - h % 8
-            hvar[ci, byte] ^= np.uint8(1 << bit)
-            calt[s] += 1 if calt[s] == 0 else -1
-        cref = N - calt
+    # keep every common site polymorphic in the panel (the reference drops
+    # monomorphic sites); rare sites always have their origin carrier
+    if rare_idx.size and (calt[rare_idx] == 0).any():
+        raise RuntimeError("rare site without a carrier")
+    mono = np.flatnonzero(((calt == 0) | (cref == 0)) & ~is_rare)
+    for s in mono:
+        ci = int(np.searchsorted(com_idx, s))
+        h = int(rng.integers(0, N))
+        hvar[ci, h // 8] ^= np.uint8(1 << (7 - h % 8))
+        calt[s] += 1 if calt[s] == 0 else -1
+    cref = N - calt
     major = (calt > cref).astype(np.uint8)
     maf = np.minimum(cref, calt) / N
     flag_common = (maf >= sparse_maf).astype(np.uint8)
@@ -266,20 +280,18 @@ def make_panel_and_targets(n_ref_haps, n_sites, region_mb, rare_frac, n_targets,
     p_alt_read = g * (1 - e) + (1 - g) * e  # P(read shows alt | genotype)
     l10_alt = np.log10(p_alt_read)
     l10_ref = np.log10(1 - p_alt_read)
-    for t in range(nt):
-        depth = rng.poisson(covs[t], L)
-        from_h1 = rng.binomial(depth, 0.5)
-        a0 = truth[t, 0].astype(np.int64)
-        a1 = truth[t, 1].astype(np.int64)
-        alt_true = (depth - from_h1) * a0 + from_h1 * a1
-        ref_true = depth - alt_true
-        alt_obs = rng.binomial(alt_true, 1 - e) + rng.binomial(ref_true, e)
-        ref_obs = depth - alt_obs
-        ll = (alt_obs[:, None] * l10_alt[None, :] + ref_obs[:, None] * l10_ref[None, :]).astype(np.float32)
-        ll -= ll.max(1, keepdims=True)
-        ph = np.minimum(np.rint(-10.0 * ll.astype(np.float64)), 255).astype(np.uint8)
-        gl[t] = ph
-        flat[t] = (ph[:, 0] == ph[:, 1]) & (ph[:, 0] == ph[:, 2])
+    depth = rng.poisson(covs[:, None].astype(np.float64), (nt, L))
+    from_h1 = rng.binomial(depth, 0.5)
+    a0 = truth[:, 0].astype(np.int64)
+    a1 = truth[:, 1].astype(np.int64)
+    alt_true = (depth - from_h1) * a0 + from_h1 * a1
+    ref_true = depth - alt_true
+    alt_obs = rng.binomial(alt_true, 1 - e) + rng.binomial(ref_true, e)
+    ref_obs = depth - alt_obs
+    ll = (alt_obs[..., None] * l10_alt + ref_obs[..., None] * l10_ref).astype(np.float32)
+    ll -= ll.max(-1, keepdims=True)
+    gl[:] = np.minimum(np.rint(-10.0 * ll.astype(np.float64)), 255).astype(np.uint8)
+    flat[:] = (gl[..., 0] == gl[..., 1]) & (gl[..., 0] == gl[..., 2])
     kp = np.rint(_draw(k, rng, nt)).astype(np.int32)
     targets = Targets(nt, np.full(nt, 2, dtype=np.int32), gl, flat, truth, covs, kp)
     params = dict(kinit=kinit, kpbwt=int(kp.max()), seed=seed)

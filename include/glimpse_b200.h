@@ -163,6 +163,27 @@ int gp_build_sparse_pbwt(const gp_panel_desc* panel, uint8_t* ypacked, int64_t* 
 /* Timing of the last gp_iteration by stage, in milliseconds (device events). */
 int gp_stage_times(gp_ctx* ctx, float* ms, int32_t n);
 
+/* Counters accumulated since the last gp_profile_reset: device time of the
+ * imputation forward-backward and phasing kernels (CUDA events around each
+ * launch on the context stream), their algorithmic work, and the number of
+ * kernels this library launched. */
+typedef struct gp_profile {
+  double impute_ms, impute_cells, impute_bytes;  /* cells = sum over launches of poly sites x states */
+  double phase_ms, phase_cells;                  /* cells = VAR sites x states x 8 hypotheses, both passes */
+  double select_ms;
+  int64_t impute_launches, phase_launches, kernel_launches;
+} gp_profile;
+int gp_profile_get(gp_ctx* ctx, gp_profile* out);
+int gp_profile_reset(gp_ctx* ctx);
+
+/* The CUDA stream the context runs on (a cudaStream_t), for callers that time
+ * or order their own work around the library's. */
+void* gp_stream(gp_ctx* ctx);
+
+/* Reset all targets to the state gp_targets_set leaves them in (haplotypes 0,
+ * no stored posteriors) without re-reading any host buffer. */
+int gp_targets_reset(gp_ctx* ctx);
+
 #ifdef __cplusplus
 }
 #endif
