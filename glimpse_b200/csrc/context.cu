@@ -319,12 +319,18 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   if ((e = p.miss.ensure((size_t)nb * L * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
   if ((e = p.seg_start.ensure((size_t)nb * (L + 2) * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
   if ((e = p.counts.ensure((size_t)nb * 3 * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.ytp.ensure((size_t)nb * L * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.ytn.ensure((size_t)nb * L * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.vflags.ensure((size_t)nb * L)) != cudaSuccess) return cuda_fail(e, "alloc vars");
   PhaseVars V;
   V.rel = p.rel.as<int32_t>();
   V.code = p.code.as<uint8_t>();
   V.seg = p.seg.as<int32_t>();
   V.miss = p.miss.as<int32_t>();
   V.seg_start = p.seg_start.as<int32_t>();
+  V.yt_prev = p.ytp.as<float>();
+  V.yt_next = p.ytn.as<float>();
+  V.flags = p.vflags.as<uint8_t>();
   V.nvar = p.counts.as<int32_t>();
   V.nseg = V.nvar + nb;
   V.nmiss = V.nvar + 2 * nb;
@@ -378,12 +384,12 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   cudaEvent_t ea;
   prof_begin(ea);
   if (launch_phase(J, d_tsel, nb, w.nstates.as<int32_t>(), w.hvar.as<uint32_t>(), w.WB, w.Kp, w.poly.as<int32_t>(),
-                   L, panel.cm, V, S, mc, cfg.seed, iteration, d_target_ids, stream) != GP_OK)
+                   w.npoly.as<int32_t>(), L, panel.cm, V, S, mc, cfg.seed, iteration, d_target_ids, stream) != GP_OK)
     return (fail(GP_E_ARG, "phasing: too many states"), GP_E_ARG);
   prof_end(ea, 1, pcells);
   launch_phase_writeback(d_tsel, nb, w.poly.as<int32_t>(), w.polyidx.as<int32_t>(), L, V, S, mc, cfg.seed, iteration,
                          d_target_ids, d_h0, d_h1, stream);
-  prof.kernel_launches += 3;
+  prof.kernel_launches += 4;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "phasing launch");
   last_phase_nseg.assign(cnt.begin() + nb, cnt.begin() + 2 * nb);
   return GP_OK;

@@ -74,11 +74,11 @@ struct ImputeWork {
 
 // Scratch of the phasing HMM.
 struct PhaseWork {
-  DevBuf rel, code, seg, miss, seg_start, counts;
+  DevBuf rel, code, seg, miss, seg_start, counts, ytp, ytn, vflags;
   DevBuf pprob, iprob, offs, pprob_sum, pprob_sumsum, iprob_sum, of1, dip, err;
   std::vector<DevBuf*> all() {
-    return {&rel, &code, &seg, &miss, &seg_start, &counts, &pprob, &iprob, &offs, &pprob_sum, &pprob_sumsum,
-            &iprob_sum, &of1, &dip, &err};
+    return {&rel, &code, &seg, &miss, &seg_start, &counts, &ytp, &ytn, &vflags, &pprob, &iprob, &offs,
+            &pprob_sum, &pprob_sumsum, &iprob_sum, &of1, &dip, &err};
   }
 };
 

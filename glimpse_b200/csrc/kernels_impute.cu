@@ -195,12 +195,34 @@ __device__ __forceinline__ void block_sum(float (&v)[NV], float (*red)[kImputeTh
 // One block per haplotype. Thread `tid` owns states k = tid + 256*j. The
 // forward pass stores every alpha row; the backward pass keeps beta in
 // registers, reads alpha back and forms the allele posteriors.
+//
+// Latency hiding: the per-site records (emissions, transitions, flags) of the
+// next 32-site block and the Hvar words of the next block are fetched while the
+// current block is processed (records go through a double-buffered shared-memory
+// stage), and the backward pass fetches the alpha row of site l-1 while it
+// works on site l. Only the per-site reduction stays on the critical path.
+struct SiteStage {
+  float4 em[2][32];
+  float2 tr[2][32];
+  uint8_t fl[2][32];
+};
+
+__device__ __forceinline__ void stage_records(SiteStage& st, int buf, int lane, int l, int np, const float4* E,
+                                              const float2* T, const uint8_t* F) {
+  if (l < np) {
+    st.em[buf][lane] = E[l];
+    st.tr[buf][lane] = T[l];
+    st.fl[buf][lane] = F[l];
+  }
+}
+
 __global__ void __launch_bounds__(kImputeThreads) k_impute_fb(
     const int32_t* __restrict__ poly, const int32_t* __restrict__ npoly, const int32_t* __restrict__ nstates,
     const uint32_t* __restrict__ hvar, const float4* __restrict__ em, const float2* __restrict__ tr,
     const uint8_t* __restrict__ fl, const int64_t* __restrict__ alpha_off, float* __restrict__ alpha_pool,
     int L, int WB, int Kp, ModelConst mc, float* __restrict__ hp) {
   __shared__ float red[2][kImputeThreads / kWarp][4];
+  __shared__ SiteStage st;
   int buf = 0;
   const int t = blockIdx.x;
   const int np = npoly[t];
@@ -213,185 +235,250 @@ __global__ void __launch_bounds__(kImputeThreads) k_impute_fb(
   const float2* T = tr + (size_t)t * L;
   const uint8_t* F = fl + (size_t)t * L;
   const int tid = threadIdx.x;
+  const bool loader = tid < 32;
   constexpr int J = kImputeStatesPerThread;
+  const int nblk = (np + 31) >> 5;
 
   float a[J];
-  uint32_t w[J];
+  uint32_t w[J], wn[J];
   float asum = 0.f;  // AlphaSum of the previous site
 
   // ---------------- forward (imputation_hmm.cpp:143-235) ----------------
-  for (int l = 0; l < np; ++l) {
-    if ((l & 31) == 0) {
+  if (loader) stage_records(st, 0, tid, tid, np, E, T, F);
 #pragma unroll
-      for (int j = 0; j < J; ++j) {
-        const int k = tid + j * kImputeThreads;
-        w[j] = (k < K) ? hv[(size_t)(l >> 5) * Kp + k] : 0u;
-      }
-    }
-    const int sh = l & 31;
-    const uint8_t f = F[l];
-    float part[1] = {0.f};
-    if (f) {  // flat or low-quality: no emission
-      if (l == 0) {
-        const float v = 1.0f / Kf;
-#pragma unroll
-        for (int j = 0; j < J; ++j) a[j] = v;
-      } else {
-        const float2 tt = T[l - 1];
-        const float fact1 = tt.x / Kf;
-        const float fact2 = tt.y / asum;
-#pragma unroll
-        for (int j = 0; j < J; ++j) {
-          const int k = tid + j * kImputeThreads;
-          if (k < K) {
-            a[j] = fmaf(a[j], fact2, fact1);
-            part[0] = __fadd_rn(part[0], a[j]);
-          }
-        }
-      }
-    } else {
-      const float4 e = E[l];
-      if (l == 0) {
-        const float fact1 = 1.0f / Kf;
-#pragma unroll
-        for (int j = 0; j < J; ++j) {
-          const int k = tid + j * kImputeThreads;
-          if (k < K) {
-            a[j] = __fmul_rn(((w[j] >> sh) & 1u) ? e.y : e.x, fact1);
-            part[0] = __fadd_rn(part[0], a[j]);
-          }
-        }
-      } else {
-        const float2 tt = T[l - 1];
-        const float fact1 = tt.x / Kf;
-        const float fact2 = tt.y / asum;
-#pragma unroll
-        for (int j = 0; j < J; ++j) {
-          const int k = tid + j * kImputeThreads;
-          if (k < K) {
-            a[j] = __fmul_rn(fmaf(a[j], fact2, fact1), ((w[j] >> sh) & 1u) ? e.y : e.x);
-            part[0] = __fadd_rn(part[0], a[j]);
-          }
-        }
-      }
-    }
-    float* row = alpha + (size_t)l * Kp;
+  for (int j = 0; j < J; ++j) {
+    const int k = tid + j * kImputeThreads;
+    w[j] = (k < K) ? hv[k] : 0u;
+  }
+  // T[l-1] of the first site of each block lives in the previous stage; keep it.
+  float2 t_prev_block = make_float2(0.f, 0.f);
+  __syncthreads();
+  for (int b = 0; b < nblk; ++b) {
+    const int cur = b & 1;
+    // prefetch block b+1
+    float4 pe; float2 pt; uint8_t pf = 0;
+    const int ln = ((b + 1) << 5) + tid;
+    const bool have_next = (b + 1 < nblk);
+    if (loader && have_next && ln < np) { pe = E[ln]; pt = T[ln]; pf = F[ln]; }
 #pragma unroll
     for (int j = 0; j < J; ++j) {
       const int k = tid + j * kImputeThreads;
-      if (k < K) row[k] = a[j];
+      wn[j] = (have_next && k < K) ? hv[(size_t)(b + 1) * Kp + k] : 0u;
     }
-    if (f && l == 0) {
-      asum = 1.0f;  // AlphaSum[0] = 1 at a flat first site (imputation_hmm.cpp:156)
-    } else {
-      block_sum<1>(part, red, buf);
-      asum = part[0];
-    }
-  }
-
-  // ---------------- backward (imputation_hmm.cpp:237-416) ----------------
-  float b[J];
-  float bsum_next = 0.f;
-  for (int l = np - 1; l >= 0; --l) {
-    if (l == np - 1 || (l & 31) == 31) {
+    const int n_in = min(32, np - (b << 5));
+    for (int i = 0; i < n_in; ++i) {
+      const int l = (b << 5) + i;
+      const uint8_t f = st.fl[cur][i];
+      const float2 tt = (i == 0) ? t_prev_block : st.tr[cur][i - 1];
+      float part[1] = {0.f};
+      if (f) {  // flat or low-quality: no emission
+        if (l == 0) {
+          const float v = 1.0f / Kf;
+#pragma unroll
+          for (int j = 0; j < J; ++j) a[j] = v;
+        } else {
+          const float fact1 = tt.x / Kf;
+          const float fact2 = tt.y / asum;
+#pragma unroll
+          for (int j = 0; j < J; ++j) {
+            const int k = tid + j * kImputeThreads;
+            if (k < K) {
+              a[j] = fmaf(a[j], fact2, fact1);
+              part[0] = __fadd_rn(part[0], a[j]);
+            }
+          }
+        }
+      } else {
+        const float4 e = st.em[cur][i];
+        if (l == 0) {
+          const float fact1 = 1.0f / Kf;
+#pragma unroll
+          for (int j = 0; j < J; ++j) {
+            const int k = tid + j * kImputeThreads;
+            if (k < K) {
+              a[j] = __fmul_rn(((w[j] >> i) & 1u) ? e.y : e.x, fact1);
+              part[0] = __fadd_rn(part[0], a[j]);
+            }
+          }
+        } else {
+          const float fact1 = tt.x / Kf;
+          const float fact2 = tt.y / asum;
+#pragma unroll
+          for (int j = 0; j < J; ++j) {
+            const int k = tid + j * kImputeThreads;
+            if (k < K) {
+              a[j] = __fmul_rn(fmaf(a[j], fact2, fact1), ((w[j] >> i) & 1u) ? e.y : e.x);
+              part[0] = __fadd_rn(part[0], a[j]);
+            }
+          }
+        }
+      }
+      float* row = alpha + (size_t)l * Kp;
 #pragma unroll
       for (int j = 0; j < J; ++j) {
         const int k = tid + j * kImputeThreads;
-        w[j] = (k < K) ? hv[(size_t)(l >> 5) * Kp + k] : 0u;
+        if (k < K) row[k] = a[j];
+      }
+      if (f && l == 0) {
+        asum = 1.0f;  // AlphaSum[0] = 1 at a flat first site (imputation_hmm.cpp:156)
+      } else {
+        block_sum<1>(part, red, buf);
+        asum = part[0];
       }
     }
-    const int sh = l & 31;
-    const uint8_t f = F[l];
-    const float* row = alpha + (size_t)l * Kp;
-    float v[3] = {0.f, 0.f, 0.f};  // prob_hid[0], prob_hid[1], betaSum
-    const float4 e = E[l];
-    const bool last = (l == np - 1);
-    if (f) {
-      if (last) {
-        const float fact1 = 1.0f / Kf;
+    t_prev_block = st.tr[cur][31 < n_in - 1 ? 31 : n_in - 1];
+    if (loader && have_next && ln < np) {
+      st.em[cur ^ 1][tid] = pe;
+      st.tr[cur ^ 1][tid] = pt;
+      st.fl[cur ^ 1][tid] = pf;
+    }
+#pragma unroll
+    for (int j = 0; j < J; ++j) w[j] = wn[j];
+    __syncthreads();
+  }
+
+  // ---------------- backward (imputation_hmm.cpp:237-416) ----------------
+  float bv[J];
+  float bsum_next = 0.f;
+  const int lastb = nblk - 1;
+  if (loader) stage_records(st, lastb & 1, tid, (lastb << 5) + tid, np, E, T, F);
+#pragma unroll
+  for (int j = 0; j < J; ++j) {
+    const int k = tid + j * kImputeThreads;
+    w[j] = (k < K) ? hv[(size_t)lastb * Kp + k] : 0u;
+  }
+  float an[J];  // alpha row of the next site to process
+  {
+    const float* row = alpha + (size_t)(np - 1) * Kp;
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      const int k = tid + j * kImputeThreads;
+      an[j] = (k < K) ? row[k] : 0.f;
+    }
+  }
+  __syncthreads();
+  for (int b = lastb; b >= 0; --b) {
+    const int cur = b & 1;
+    float4 pe; float2 pt; uint8_t pf = 0;
+    const bool have_next = b > 0;
+    const int ln = ((b - 1) << 5) + tid;
+    if (loader && have_next) { pe = E[ln]; pt = T[ln]; pf = F[ln]; }
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      const int k = tid + j * kImputeThreads;
+      wn[j] = (have_next && k < K) ? hv[(size_t)(b - 1) * Kp + k] : 0u;
+    }
+    const int n_in = min(32, np - (b << 5));
+    for (int i = n_in - 1; i >= 0; --i) {
+      const int l = (b << 5) + i;
+      float av[J];
+#pragma unroll
+      for (int j = 0; j < J; ++j) av[j] = an[j];
+      if (l > 0) {
+        const float* row = alpha + (size_t)(l - 1) * Kp;
 #pragma unroll
         for (int j = 0; j < J; ++j) {
           const int k = tid + j * kImputeThreads;
-          if (k < K) {
-            const float av = row[k];
-            if ((w[j] >> sh) & 1u) v[1] = __fadd_rn(v[1], av); else v[0] = __fadd_rn(v[0], av);
-            b[j] = fact1;
+          an[j] = (k < K) ? row[k] : 0.f;
+        }
+      }
+      const uint8_t f = st.fl[cur][i];
+      float v[3] = {0.f, 0.f, 0.f};  // prob_hid[0], prob_hid[1], betaSum
+      const float4 e = st.em[cur][i];
+      const bool last = (l == np - 1);
+      if (f) {
+        if (last) {
+          const float fact1 = 1.0f / Kf;
+#pragma unroll
+          for (int j = 0; j < J; ++j) {
+            const int k = tid + j * kImputeThreads;
+            if (k < K) {
+              if ((w[j] >> i) & 1u) v[1] = __fadd_rn(v[1], av[j]); else v[0] = __fadd_rn(v[0], av[j]);
+              bv[j] = fact1;
+            }
+          }
+        } else {
+          const float2 tt = st.tr[cur][i];
+          const float fact1 = tt.x / Kf;
+          const float fact2 = tt.y / bsum_next;
+#pragma unroll
+          for (int j = 0; j < J; ++j) {
+            const int k = tid + j * kImputeThreads;
+            if (k < K) {
+              const float pc = fmaf(bv[j], fact2, fact1);
+              const float dot = __fmul_rn(av[j], pc);
+              if ((w[j] >> i) & 1u) v[1] = __fadd_rn(v[1], dot); else v[0] = __fadd_rn(v[0], dot);
+              v[2] = __fadd_rn(v[2], pc);
+              bv[j] = pc;
+            }
           }
         }
       } else {
-        const float2 tt = T[l];
-        const float fact1 = tt.x / Kf;
-        const float fact2 = tt.y / bsum_next;
+        if (last) {
+          const float fact1 = 1.0f / Kf;
 #pragma unroll
-        for (int j = 0; j < J; ++j) {
-          const int k = tid + j * kImputeThreads;
-          if (k < K) {
-            const float pc = fmaf(b[j], fact2, fact1);
-            const float dot = __fmul_rn(row[k], pc);
-            if ((w[j] >> sh) & 1u) v[1] = __fadd_rn(v[1], dot); else v[0] = __fadd_rn(v[0], dot);
-            v[2] = __fadd_rn(v[2], pc);
-            b[j] = pc;
+          for (int j = 0; j < J; ++j) {
+            const int k = tid + j * kImputeThreads;
+            if (k < K) {
+              const bool bit = (w[j] >> i) & 1u;
+              if (bit) v[1] = __fadd_rn(v[1], av[j]); else v[0] = __fadd_rn(v[0], av[j]);
+              const float pn = __fmul_rn(bit ? e.y : e.x, fact1);
+              v[2] = __fadd_rn(v[2], pn);
+              bv[j] = pn;
+            }
+          }
+        } else {
+          const float2 tt = st.tr[cur][i];
+          const float fact1 = tt.x / Kf;
+          const float fact2 = tt.y / bsum_next;
+#pragma unroll
+          for (int j = 0; j < J; ++j) {
+            const int k = tid + j * kImputeThreads;
+            if (k < K) {
+              const bool bit = (w[j] >> i) & 1u;
+              const float pc = fmaf(bv[j], fact2, fact1);
+              const float dot = __fmul_rn(av[j], pc);
+              const float pn = __fmul_rn(pc, bit ? e.y : e.x);
+              if (bit) v[1] = __fadd_rn(v[1], dot); else v[0] = __fadd_rn(v[0], dot);
+              v[2] = __fadd_rn(v[2], pn);
+              bv[j] = pn;
+            }
           }
         }
       }
-    } else {
-      if (last) {
-        const float fact1 = 1.0f / Kf;
-#pragma unroll
-        for (int j = 0; j < J; ++j) {
-          const int k = tid + j * kImputeThreads;
-          if (k < K) {
-            const float av = row[k];
-            const bool bit = (w[j] >> sh) & 1u;
-            if (bit) v[1] = __fadd_rn(v[1], av); else v[0] = __fadd_rn(v[0], av);
-            const float pn = __fmul_rn(bit ? e.y : e.x, fact1);
-            v[2] = __fadd_rn(v[2], pn);
-            b[j] = pn;
-          }
+      block_sum<3>(v, red, buf);
+      float bsum = v[2];
+      float po0, po1;
+      if (f) {
+        if (last) bsum = 1.0f;
+        po0 = fmaf(v[0], mc.ee_imp, __fmul_rn(v[1], mc.ed_imp));
+        po1 = fmaf(v[0], mc.ed_imp, __fmul_rn(v[1], mc.ee_imp));
+        if (!(f & 1)) {
+          po0 = __fmul_rn(po0, e.z);
+          po1 = __fmul_rn(po1, e.w);
         }
       } else {
-        const float2 tt = T[l];
-        const float fact1 = tt.x / Kf;
-        const float fact2 = tt.y / bsum_next;
+        const float ph0 = v[0] / e.x;
+        const float ph1 = v[1] / e.y;
+        po0 = __fmul_rn(fmaf(ph0, mc.ee_imp, __fmul_rn(ph1, mc.ed_imp)), e.z);
+        po1 = __fmul_rn(fmaf(ph0, mc.ed_imp, __fmul_rn(ph1, mc.ee_imp)), e.w);
+      }
+      if (tid == 0) {
+        const int s = poly[(size_t)t * L + l];
+        const float den = __fadd_rn(po0, po1);
+        hp[(size_t)t * 2 * L + 2 * s] = po0 / den;
+        hp[(size_t)t * 2 * L + 2 * s + 1] = po1 / den;
+      }
+      bsum_next = bsum;
+    }
+    if (loader && have_next) {
+      st.em[cur ^ 1][tid] = pe;
+      st.tr[cur ^ 1][tid] = pt;
+      st.fl[cur ^ 1][tid] = pf;
+    }
 #pragma unroll
-        for (int j = 0; j < J; ++j) {
-          const int k = tid + j * kImputeThreads;
-          if (k < K) {
-            const bool bit = (w[j] >> sh) & 1u;
-            const float pc = fmaf(b[j], fact2, fact1);
-            const float dot = __fmul_rn(row[k], pc);
-            const float pn = __fmul_rn(pc, bit ? e.y : e.x);
-            if (bit) v[1] = __fadd_rn(v[1], dot); else v[0] = __fadd_rn(v[0], dot);
-            v[2] = __fadd_rn(v[2], pn);
-            b[j] = pn;
-          }
-        }
-      }
-    }
-    block_sum<3>(v, red, buf);
-    float bsum = v[2];
-    float po0, po1;
-    if (f) {
-      if (last) bsum = 1.0f;
-      po0 = fmaf(v[0], mc.ee_imp, __fmul_rn(v[1], mc.ed_imp));
-      po1 = fmaf(v[0], mc.ed_imp, __fmul_rn(v[1], mc.ee_imp));
-      if (!(f & 1)) {
-        po0 = __fmul_rn(po0, e.z);
-        po1 = __fmul_rn(po1, e.w);
-      }
-    } else {
-      const float ph0 = v[0] / e.x;
-      const float ph1 = v[1] / e.y;
-      po0 = __fmul_rn(fmaf(ph0, mc.ee_imp, __fmul_rn(ph1, mc.ed_imp)), e.z);
-      po1 = __fmul_rn(fmaf(ph0, mc.ed_imp, __fmul_rn(ph1, mc.ee_imp)), e.w);
-    }
-    if (tid == 0) {
-      const int s = poly[(size_t)t * L + l];
-      const float den = __fadd_rn(po0, po1);
-      hp[(size_t)t * 2 * L + 2 * s] = po0 / den;
-      hp[(size_t)t * 2 * L + 2 * s + 1] = po1 / den;
-    }
-    bsum_next = bsum;
+    for (int j = 0; j < J; ++j) w[j] = wn[j];
+    __syncthreads();
   }
 }
 

@@ -113,6 +113,34 @@ __global__ void k_build_vars(const int32_t* __restrict__ poly, const int32_t* __
   }
 }
 
+// Per-entry transitions (conditioning_set.h:101-105, as getTransition is called
+// in phasing_hmm.cpp:152,201 and phasing_hmm.h:381) and segment flags.
+__device__ __forceinline__ float transition(const double* __restrict__ cm, int prev, int next, const ModelConst& mc);
+
+__global__ void k_var_records(const int32_t* __restrict__ tsel, const int32_t* __restrict__ poly, int L,
+                              const double* __restrict__ cm, ModelConst mc, PhaseVars V) {
+  const int b = blockIdx.y;
+  const int t = tsel ? tsel[b] : b;
+  const int nv = V.nvar[b];
+  const int32_t* pl = poly + (size_t)t * L;
+  const int32_t* vrel = V.rel + (size_t)b * L;
+  const int32_t* vseg = V.seg + (size_t)b * L;
+  const int32_t* sstart = V.seg_start + (size_t)b * (L + 2);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x) {
+    const int s = pl[vrel[i]];
+    float yn = 0.f;
+    if (i + 1 < nv) yn = transition(cm, s, pl[vrel[i + 1]], mc);
+    V.yt_next[(size_t)b * L + i] = yn;
+    float yp = 0.f;
+    if (i > 0) yp = transition(cm, pl[vrel[i - 1]], s, mc);
+    V.yt_prev[(size_t)b * L + i] = yp;
+    const int seg = vseg[i];
+    const int locus = i - sstart[seg];
+    const int seglen = sstart[seg + 1] - sstart[seg];
+    V.flags[(size_t)b * L + i] = (uint8_t)((locus == 0 ? 1 : 0) | (locus == seglen - 1 ? 2 : 0));
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Block reduction of 8 values (one per hypothesis).
 // Within a warp a reduce-scatter leaves lane L with the warp sum of value
@@ -249,28 +277,91 @@ __device__ __forceinline__ void site_update(float (&prob)[J][8], const float (&s
   sumT = hadd8(sumH);
 }
 
+// VAR records of 32 consecutive entries, double-buffered in shared memory.
+struct VarStage {
+  int32_t l[2][32];
+  int32_t seg[2][32];
+  int32_t miss[2][32];
+  float ytp[2][32];
+  float ytn[2][32];
+  uint8_t code[2][32];
+  uint8_t flags[2][32];
+};
+
+struct VarRec {
+  int32_t l, seg, miss;
+  float ytp, ytn;
+  uint8_t code, flags;
+};
+
+__device__ __forceinline__ VarRec load_rec(const PhaseVars& V, size_t base, int i) {
+  VarRec r;
+  r.l = V.rel[base + i];
+  r.seg = V.seg[base + i];
+  r.miss = V.miss[base + i];
+  r.ytp = V.yt_prev[base + i];
+  r.ytn = V.yt_next[base + i];
+  r.code = V.code[base + i];
+  r.flags = V.flags[base + i];
+  return r;
+}
+
+__device__ __forceinline__ void put_rec(VarStage& st, int buf, int lane, const VarRec& r) {
+  st.l[buf][lane] = r.l;
+  st.seg[buf][lane] = r.seg;
+  st.miss[buf][lane] = r.miss;
+  st.ytp[buf][lane] = r.ytp;
+  st.ytn[buf][lane] = r.ytn;
+  st.code[buf][lane] = r.code;
+  st.flags[buf][lane] = r.flags;
+}
+
+// Hvar words of the poly block holding the current site, with the adjacent
+// block (in sweep direction) fetched ahead.
+template <int J>
+struct WordCache {
+  uint32_t w[J], wn[J];
+  int cur = -1, nxt = -1;
+  __device__ __forceinline__ void fetch(uint32_t (&dst)[J], const uint32_t* hv, int blk, int nblk, int Kp, int K,
+                                        int tid) {
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      const int k = tid + j * PT;
+      dst[j] = (blk >= 0 && blk < nblk && k < K) ? hv[(size_t)blk * Kp + k] : 0u;
+    }
+  }
+  __device__ __forceinline__ void need(int blk, int dir, const uint32_t* hv, int nblk, int Kp, int K, int tid) {
+    if (blk == cur) return;
+    if (blk == nxt) {
+#pragma unroll
+      for (int j = 0; j < J; ++j) w[j] = wn[j];
+    } else {
+      fetch(w, hv, blk, nblk, Kp, K, tid);
+    }
+    cur = blk;
+    nxt = blk + dir;
+    fetch(wn, hv, nxt, nblk, Kp, K, tid);
+  }
+};
+
 template <int J>
 __global__ void __launch_bounds__(PT) k_phase(const int32_t* __restrict__ tsel, const int32_t* __restrict__ nstates,
-                                              const uint32_t* __restrict__ hvar, int WB, int Kp,
-                                              const int32_t* __restrict__ poly, int L,
-                                              const double* __restrict__ cm, PhaseVars V, PhaseStore S,
-                                              ModelConst mc, uint64_t seed, int iteration,
-                                              const int32_t* __restrict__ target_ids) {
+                                              const int32_t* __restrict__ npoly, const uint32_t* __restrict__ hvar,
+                                              int WB, int Kp, int L, PhaseVars V, PhaseStore S, ModelConst mc,
+                                              uint64_t seed, int iteration, const int32_t* __restrict__ target_ids) {
   __shared__ PhaseShared sm;
+  __shared__ VarStage vs;
   int buf = 0;
   const int b = blockIdx.x;
   const int t = tsel ? tsel[b] : b;
   const int K = nstates[t];
   const int nv = V.nvar[b];
   const int tid = threadIdx.x;
+  const bool loader = tid < 32;
   if (tid == 0) sm.err = 0;
   const uint32_t* hv = hvar + (size_t)t * WB * Kp;
-  const int32_t* vrel = V.rel + (size_t)b * L;
-  const uint8_t* vcode = V.code + (size_t)b * L;
-  const int32_t* vseg = V.seg + (size_t)b * L;
-  const int32_t* vmiss = V.miss + (size_t)b * L;
-  const int32_t* sstart = V.seg_start + (size_t)b * (L + 2);
-  const int32_t* pl = poly + (size_t)t * L;
+  const int nblk_poly = (npoly[t] + 31) >> 5;
+  const size_t vbase = (size_t)b * L;
   float* PP = S.pprob + S.pprob_off[b];            // [nseg][K][8]
   float* PPS = S.pprob_sum + (size_t)b * (L + 2) * 8;  // [nseg][8]
   float* PPSS = S.pprob_sumsum + (size_t)b * (L + 2);  // [nseg]
@@ -279,75 +370,70 @@ __global__ void __launch_bounds__(PT) k_phase(const int32_t* __restrict__ tsel, 
   float* OF1 = S.of1 + (size_t)b * L * 8;           // [nmiss][8]
   int32_t* dip = S.dip + (size_t)b * (L + 2);
   const uint32_t rng_target = target_ids ? (uint32_t)target_ids[b] : (uint32_t)t;
+  const int nvb = (nv + 31) >> 5;
 
   float prob[J][8];
   float sumk[J];
-  uint32_t w[J];
   float sumH[8];
   float sumT = 0.f;
 #pragma unroll
   for (int j = 0; j < J; ++j) sumk[j] = 0.f;
-  int loaded_block = -1;
+  WordCache<J> wc;
 
-  auto load_bits = [&](int l) {
-    const int blk = l >> 5;
-    if (blk != loaded_block) {
-      loaded_block = blk;
-#pragma unroll
-      for (int j = 0; j < J; ++j) {
-        const int k = tid + j * PT;
-        w[j] = (k < K) ? hv[(size_t)blk * Kp + k] : 0u;
-      }
-    }
-  };
   auto do_sumk = [&]() {
 #pragma unroll
     for (int j = 0; j < J; ++j) sumk[j] = hadd8(prob[j]);
   };
+  auto store_rows = [&](float* dst) {
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      const int k = tid + j * PT;
+      if (k < K) {
+        float4* d4 = reinterpret_cast<float4*>(dst + (size_t)k * 8);
+        d4[0] = make_float4(prob[j][0], prob[j][1], prob[j][2], prob[j][3]);
+        d4[1] = make_float4(prob[j][4], prob[j][5], prob[j][6], prob[j][7]);
+      }
+    }
+  };
 
   // ---------------- backward (phasing_hmm.cpp:193-245) ----------------
-  for (int i = nv - 1; i >= 0; --i) {
-    const int l = vrel[i];
-    load_bits(l);
-    const int code = vcode[i];
-    const int typ = code & 7, alt = (code >> 3) & 1;
-    const int seg = vseg[i];
-    const int locus = i - sstart[seg];
-    const int seglen = sstart[seg + 1] - sstart[seg];
-    float yt = 0.f;
-    if (i < nv - 1) yt = transition(cm, pl[l], pl[vrel[i + 1]], mc);
-    const float nt = 1.0f - yt;
-    const int mode = (i == nv - 1) ? 0 : ((locus != seglen - 1) ? 1 : 2);
-    site_update<J>(prob, sumk, w, l & 31, K, tid, typ, alt, mode, yt, nt, mc, sumH, sumT, sm.red, buf);
-    if (locus == 0) {
-      do_sumk();
-      float* dst = PP + (size_t)seg * K * 8;
-#pragma unroll
-      for (int j = 0; j < J; ++j) {
-        const int k = tid + j * PT;
-        if (k < K) {
-          float4* d4 = reinterpret_cast<float4*>(dst + (size_t)k * 8);
-          d4[0] = make_float4(prob[j][0], prob[j][1], prob[j][2], prob[j][3]);
-          d4[1] = make_float4(prob[j][4], prob[j][5], prob[j][6], prob[j][7]);
-        }
+  if (nvb > 0) {
+    const int lb = nvb - 1;
+    if (loader && (lb << 5) + tid < nv) put_rec(vs, lb & 1, tid, load_rec(V, vbase, (lb << 5) + tid));
+  }
+  __syncthreads();
+  for (int vb = nvb - 1; vb >= 0; --vb) {
+    const int cur = vb & 1;
+    VarRec pre;
+    const bool have_next = vb > 0;
+    if (loader && have_next) pre = load_rec(V, vbase, ((vb - 1) << 5) + tid);
+    const int n_in = min(32, nv - (vb << 5));
+    for (int ii = n_in - 1; ii >= 0; --ii) {
+      const int i = (vb << 5) + ii;
+      const int l = vs.l[cur][ii];
+      wc.need(l >> 5, -1, hv, nblk_poly, Kp, K, tid);
+      const int code = vs.code[cur][ii];
+      const int typ = code & 7, alt = (code >> 3) & 1;
+      const int seg = vs.seg[cur][ii];
+      const int fl = vs.flags[cur][ii];
+      const float yt = vs.ytn[cur][ii];
+      const float nt = 1.0f - yt;
+      const int mode = (i == nv - 1) ? 0 : ((fl & 2) ? 2 : 1);
+      site_update<J>(prob, sumk, wc.w, l & 31, K, tid, typ, alt, mode, yt, nt, mc, sumH, sumT, sm.red, buf);
+      if (fl & 1) {
+        do_sumk();
+        store_rows(PP + (size_t)seg * K * 8);
+        if (tid < 8) PPS[seg * 8 + tid] = sumH[tid];
+        if (tid == 0) PPSS[seg] = sumT;
       }
-      if (tid < 8) PPS[seg * 8 + tid] = sumH[tid];
-      if (tid == 0) PPSS[seg] = sumT;
-    }
-    if (typ == VT_FLAT) {
-      const int m = vmiss[i];
-      float* dst = IP + (size_t)m * K * 8;
-#pragma unroll
-      for (int j = 0; j < J; ++j) {
-        const int k = tid + j * PT;
-        if (k < K) {
-          float4* d4 = reinterpret_cast<float4*>(dst + (size_t)k * 8);
-          d4[0] = make_float4(prob[j][0], prob[j][1], prob[j][2], prob[j][3]);
-          d4[1] = make_float4(prob[j][4], prob[j][5], prob[j][6], prob[j][7]);
-        }
+      if (typ == VT_FLAT) {
+        const int m = vs.miss[cur][ii];
+        store_rows(IP + (size_t)m * K * 8);
+        if (tid < 8) IPS[m * 8 + tid] = sumH[tid];
       }
-      if (tid < 8) IPS[m * 8 + tid] = sumH[tid];
     }
+    if (loader && have_next) put_rec(vs, cur ^ 1, tid, pre);
+    __syncthreads();
   }
   __syncthreads();
 
@@ -375,121 +461,131 @@ __global__ void __launch_bounds__(PT) k_phase(const int32_t* __restrict__ tsel, 
   __syncthreads();
 
   // ---------------- forward (phasing_hmm.cpp:142-191) ----------------
-  loaded_block = -1;
-  for (int i = 0; i < nv; ++i) {
-    const int l = vrel[i];
-    load_bits(l);
-    const int code = vcode[i];
-    const int typ = code & 7, alt = (code >> 3) & 1;
-    const int seg = vseg[i];
-    const int locus = i - sstart[seg];
-    const int seglen = sstart[seg + 1] - sstart[seg];
-    float yt = 0.f;
-    if (i) yt = transition(cm, pl[vrel[i - 1]], pl[l], mc);
-    const float nt = 1.0f - yt;
-    const int mode = (i == 0) ? 0 : ((locus != 0) ? 1 : 2);
-    site_update<J>(prob, sumk, w, l & 31, K, tid, typ, alt, mode, yt, nt, mc, sumH, sumT, sm.red, buf);
-    const bool seg_end = (locus == seglen - 1);
-    if (seg_end) do_sumk();
-    if (seg_end && i != nv - 1) {
-      // TRANS_HAP (phasing_hmm.h:376-397)
-      const float yt2 = transition(cm, pl[l], pl[vrel[i + 1]], mc);
-      const float nt2 = 1.0f - yt2;
-      const float fact2 = nt2 / sumT;
-      const float* nxt = PP + (size_t)(seg + 1) * K * 8;
-      float sumHP = 0.f;
+  wc.cur = wc.nxt = -1;
+  if (nvb > 0 && loader && tid < nv) put_rec(vs, 0, tid, load_rec(V, vbase, tid));
+  __syncthreads();
+  for (int vb = 0; vb < nvb; ++vb) {
+    const int cur = vb & 1;
+    VarRec pre;
+    const bool have_next = vb + 1 < nvb;
+    if (loader && have_next && ((vb + 1) << 5) + tid < nv) pre = load_rec(V, vbase, ((vb + 1) << 5) + tid);
+    const int n_in = min(32, nv - (vb << 5));
+    for (int ii = 0; ii < n_in; ++ii) {
+      const int i = (vb << 5) + ii;
+      const int l = vs.l[cur][ii];
+      wc.need(l >> 5, 1, hv, nblk_poly, Kp, K, tid);
+      const int code = vs.code[cur][ii];
+      const int typ = code & 7, alt = (code >> 3) & 1;
+      const int seg = vs.seg[cur][ii];
+      const int fl = vs.flags[cur][ii];
+      const float yt = vs.ytp[cur][ii];
+      const float nt = 1.0f - yt;
+      const int mode = (i == 0) ? 0 : ((fl & 1) ? 2 : 1);
+      site_update<J>(prob, sumk, wc.w, l & 31, K, tid, typ, alt, mode, yt, nt, mc, sumH, sumT, sm.red, buf);
+      const bool seg_end = (fl & 2) != 0;
+      if (seg_end) do_sumk();
+      if (seg_end && i != nv - 1) {
+        // TRANS_HAP (phasing_hmm.h:376-397)
+        const float yt2 = vs.ytn[cur][ii];
+        const float nt2 = 1.0f - yt2;
+        const float fact2 = nt2 / sumT;
+        const float* nxt = PP + (size_t)(seg + 1) * K * 8;
+        float sumHP = 0.f;
 #pragma unroll
-      for (int h1 = 0; h1 < 8; ++h1) {
-        const float fact1 = __fmul_rn(sumH[h1] / sumT, yt2) / (float)K;
-        float acc[8];
+        for (int h1 = 0; h1 < 8; ++h1) {
+          const float fact1 = __fmul_rn(sumH[h1] / sumT, yt2) / (float)K;
+          float acc[8];
 #pragma unroll
-        for (int h2 = 0; h2 < 8; ++h2) acc[h2] = 0.f;
+          for (int h2 = 0; h2 < 8; ++h2) acc[h2] = 0.f;
+#pragma unroll
+          for (int j = 0; j < J; ++j) {
+            const int k = tid + j * PT;
+            if (k < K) {
+              const float p0 = fmaf(prob[j][h1], fact2, fact1);
+              const float4* s4 = reinterpret_cast<const float4*>(nxt + (size_t)k * 8);
+              const float4 x = s4[0], y = s4[1];
+              acc[0] = fmaf(p0, x.x, acc[0]); acc[1] = fmaf(p0, x.y, acc[1]);
+              acc[2] = fmaf(p0, x.z, acc[2]); acc[3] = fmaf(p0, x.w, acc[3]);
+              acc[4] = fmaf(p0, y.x, acc[4]); acc[5] = fmaf(p0, y.y, acc[5]);
+              acc[6] = fmaf(p0, y.z, acc[6]); acc[7] = fmaf(p0, y.w, acc[7]);
+            }
+          }
+          float tot[8];
+          block_sum8(acc, sm.red, buf, tot);
+          if (tid == 0)
+#pragma unroll
+            for (int h2 = 0; h2 < 8; ++h2) sm.hprobs[h1 * 8 + h2] = tot[h2];
+          sumHP = __fadd_rn(sumHP, hadd8(tot));
+        }
+        // SAMPLE_DIP (phasing_hmm.h:400-411)
+        if (tid == 0) {
+          const bool bad1 = isnan(sumHP) || isinf(sumHP) || sumHP < 1.17549435e-38f;
+          const int prev = sm.dip;
+          float dp[8];
+          float sd = 0.f;
+          for (int d = 0; d < 8; ++d) {
+            dp[d] = __fmul_rn(sm.hprobs[prev * 8 + d] / sumHP, sm.hprobs[(7 - prev) * 8 + (7 - d)] / sumHP);
+            sd = __fadd_rn(sd, dp[d]);
+          }
+          const bool bad2 = isnan(sd) || isinf(sd) || sd < 1.17549435e-38f;
+          int nd = prev;
+          if (bad1 || bad2) {
+            sm.err = 1;
+          } else {
+            const float u = __fmul_rn(canonical_float(stream_word(seed, RNG_PHASE, iteration, rng_target,
+                                                                  (uint64_t)(seg + 1))), sd);
+            float cs = dp[0];
+            nd = 7;
+            for (int d = 0; d < 7; ++d) {
+              if (u <= cs) { nd = d; break; }
+              cs = __fadd_rn(cs, dp[d + 1]);
+            }
+          }
+          dip[seg + 1] = nd;
+          sm.dip = nd;
+        }
+        __syncthreads();
+      }
+      if (typ == VT_FLAT) {
+        // IMPUTE_FLAT_HET (phasing_hmm.h:414-447)
+        const int m = vs.miss[cur][ii];
+        const float* src = IP + (size_t)m * K * 8;
+        float sR[8], sL[8];
+#pragma unroll
+        for (int h = 0; h < 8; ++h) {
+          sR[h] = 1.0f / IPS[m * 8 + h];
+          sL[h] = 1.0f / sumH[h];
+        }
+        float s0[8], s1[8];
+#pragma unroll
+        for (int h = 0; h < 8; ++h) s0[h] = s1[h] = 0.f;
 #pragma unroll
         for (int j = 0; j < J; ++j) {
           const int k = tid + j * PT;
           if (k < K) {
-            const float p0 = fmaf(prob[j][h1], fact2, fact1);
-            const float4* s4 = reinterpret_cast<const float4*>(nxt + (size_t)k * 8);
+            const int bit = (wc.w[j] >> (l & 31)) & 1u;
+            const float4* s4 = reinterpret_cast<const float4*>(src + (size_t)k * 8);
             const float4 x = s4[0], y = s4[1];
-            acc[0] = fmaf(p0, x.x, acc[0]); acc[1] = fmaf(p0, x.y, acc[1]);
-            acc[2] = fmaf(p0, x.z, acc[2]); acc[3] = fmaf(p0, x.w, acc[3]);
-            acc[4] = fmaf(p0, y.x, acc[4]); acc[5] = fmaf(p0, y.y, acc[5]);
-            acc[6] = fmaf(p0, y.z, acc[6]); acc[7] = fmaf(p0, y.w, acc[7]);
+            const float ip[8] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
+#pragma unroll
+            for (int h = 0; h < 8; ++h) {
+              const float p1 = __fmul_rn(ip[h], sR[h]);
+              const float p2 = __fmul_rn(prob[j][h], sL[h]);
+              if (bit) s1[h] = fmaf(p1, p2, s1[h]); else s0[h] = fmaf(p1, p2, s0[h]);
+            }
           }
         }
-        float tot[8];
-        block_sum8(acc, sm.red, buf, tot);
-        if (tid == 0)
-#pragma unroll
-          for (int h2 = 0; h2 < 8; ++h2) sm.hprobs[h1 * 8 + h2] = tot[h2];
-        sumHP = __fadd_rn(sumHP, hadd8(tot));
-      }
-      // SAMPLE_DIP (phasing_hmm.h:400-411)
-      if (tid == 0) {
-        const bool bad1 = isnan(sumHP) || isinf(sumHP) || sumHP < 1.17549435e-38f;
-        const int prev = sm.dip;
-        float dp[8];
-        float sd = 0.f;
-        for (int d = 0; d < 8; ++d) {
-          dp[d] = __fmul_rn(sm.hprobs[prev * 8 + d] / sumHP, sm.hprobs[(7 - prev) * 8 + (7 - d)] / sumHP);
-          sd = __fadd_rn(sd, dp[d]);
+        float t0[8], t1[8];
+        block_sum8(s0, sm.red, buf, t0);
+        block_sum8(s1, sm.red, buf, t1);
+        if (tid < 8) {
+          const float r = t1[tid] / __fadd_rn(t0[tid], t1[tid]);
+          OF1[m * 8 + tid] = fmaxf(0.0f, fminf(1.0f, r));
         }
-        const bool bad2 = isnan(sd) || isinf(sd) || sd < 1.17549435e-38f;
-        int nd = prev;
-        if (bad1 || bad2) {
-          sm.err = 1;
-        } else {
-          const float u = __fmul_rn(canonical_float(stream_word(seed, RNG_PHASE, iteration, rng_target,
-                                                                (uint64_t)(seg + 1))), sd);
-          float cs = dp[0];
-          nd = 7;
-          for (int d = 0; d < 7; ++d) {
-            if (u <= cs) { nd = d; break; }
-            cs = __fadd_rn(cs, dp[d + 1]);
-          }
-        }
-        dip[seg + 1] = nd;
-        sm.dip = nd;
-      }
-      __syncthreads();
-    }
-    if (typ == VT_FLAT) {
-      // IMPUTE_FLAT_HET (phasing_hmm.h:414-447)
-      const int m = vmiss[i];
-      const float* src = IP + (size_t)m * K * 8;
-      float sR[8], sL[8];
-#pragma unroll
-      for (int h = 0; h < 8; ++h) {
-        sR[h] = 1.0f / IPS[m * 8 + h];
-        sL[h] = 1.0f / sumH[h];
-      }
-      float s0[8], s1[8];
-#pragma unroll
-      for (int h = 0; h < 8; ++h) s0[h] = s1[h] = 0.f;
-#pragma unroll
-      for (int j = 0; j < J; ++j) {
-        const int k = tid + j * PT;
-        if (k < K) {
-          const int bit = (w[j] >> (l & 31)) & 1u;
-          const float4* s4 = reinterpret_cast<const float4*>(src + (size_t)k * 8);
-          const float4 x = s4[0], y = s4[1];
-          const float ip[8] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
-#pragma unroll
-          for (int h = 0; h < 8; ++h) {
-            const float p1 = __fmul_rn(ip[h], sR[h]);
-            const float p2 = __fmul_rn(prob[j][h], sL[h]);
-            if (bit) s1[h] = fmaf(p1, p2, s1[h]); else s0[h] = fmaf(p1, p2, s0[h]);
-          }
-        }
-      }
-      float t0[8], t1[8];
-      block_sum8(s0, sm.red, buf, t0);
-      block_sum8(s1, sm.red, buf, t1);
-      if (tid < 8) {
-        const float r = t1[tid] / __fadd_rn(t0[tid], t1[tid]);
-        OF1[m * 8 + tid] = fmaxf(0.0f, fminf(1.0f, r));
       }
     }
+    if (loader && have_next && ((vb + 1) << 5) + tid < nv) put_rec(vs, cur ^ 1, tid, pre);
+    __syncthreads();
   }
   if (tid == 0) S.err[b] = sm.err;
 }
@@ -587,17 +683,18 @@ void launch_build_vars(const int32_t* tsel, int nb, const int32_t* poly, const i
 }
 
 int launch_phase(int J, const int32_t* tsel, int nb, const int32_t* nstates, const uint32_t* hvar, int WB, int Kp,
-                 const int32_t* poly, int L, const double* cm, PhaseVars V, PhaseStore S, const ModelConst& mc,
-                 uint64_t seed, int iteration, const int32_t* target_ids, cudaStream_t s) {
+                 const int32_t* poly, const int32_t* npoly, int L, const double* cm, PhaseVars V, PhaseStore S,
+                 const ModelConst& mc, uint64_t seed, int iteration, const int32_t* target_ids, cudaStream_t s) {
+  k_var_records<<<dim3(32, nb), 256, 0, s>>>(tsel, poly, L, cm, mc, V);
   switch (J) {
-    case 1: k_phase<1><<<nb, PT, 0, s>>>(tsel, nstates, hvar, WB, Kp, poly, L, cm, V, S, mc, seed, iteration, target_ids); break;
-    case 2: k_phase<2><<<nb, PT, 0, s>>>(tsel, nstates, hvar, WB, Kp, poly, L, cm, V, S, mc, seed, iteration, target_ids); break;
-    case 3: k_phase<3><<<nb, PT, 0, s>>>(tsel, nstates, hvar, WB, Kp, poly, L, cm, V, S, mc, seed, iteration, target_ids); break;
-    case 4: k_phase<4><<<nb, PT, 0, s>>>(tsel, nstates, hvar, WB, Kp, poly, L, cm, V, S, mc, seed, iteration, target_ids); break;
-    case 5: k_phase<5><<<nb, PT, 0, s>>>(tsel, nstates, hvar, WB, Kp, poly, L, cm, V, S, mc, seed, iteration, target_ids); break;
-    case 6: k_phase<6><<<nb, PT, 0, s>>>(tsel, nstates, hvar, WB, Kp, poly, L, cm, V, S, mc, seed, iteration, target_ids); break;
-    case 7: k_phase<7><<<nb, PT, 0, s>>>(tsel, nstates, hvar, WB, Kp, poly, L, cm, V, S, mc, seed, iteration, target_ids); break;
-    case 8: k_phase<8><<<nb, PT, 0, s>>>(tsel, nstates, hvar, WB, Kp, poly, L, cm, V, S, mc, seed, iteration, target_ids); break;
+    case 1: k_phase<1><<<nb, PT, 0, s>>>(tsel, nstates, npoly, hvar, WB, Kp, L, V, S, mc, seed, iteration, target_ids); break;
+    case 2: k_phase<2><<<nb, PT, 0, s>>>(tsel, nstates, npoly, hvar, WB, Kp, L, V, S, mc, seed, iteration, target_ids); break;
+    case 3: k_phase<3><<<nb, PT, 0, s>>>(tsel, nstates, npoly, hvar, WB, Kp, L, V, S, mc, seed, iteration, target_ids); break;
+    case 4: k_phase<4><<<nb, PT, 0, s>>>(tsel, nstates, npoly, hvar, WB, Kp, L, V, S, mc, seed, iteration, target_ids); break;
+    case 5: k_phase<5><<<nb, PT, 0, s>>>(tsel, nstates, npoly, hvar, WB, Kp, L, V, S, mc, seed, iteration, target_ids); break;
+    case 6: k_phase<6><<<nb, PT, 0, s>>>(tsel, nstates, npoly, hvar, WB, Kp, L, V, S, mc, seed, iteration, target_ids); break;
+    case 7: k_phase<7><<<nb, PT, 0, s>>>(tsel, nstates, npoly, hvar, WB, Kp, L, V, S, mc, seed, iteration, target_ids); break;
+    case 8: k_phase<8><<<nb, PT, 0, s>>>(tsel, nstates, npoly, hvar, WB, Kp, L, V, S, mc, seed, iteration, target_ids); break;
     default: return GP_E_ARG;
   }
   return GP_OK;

@@ -17,6 +17,9 @@ struct PhaseVars {
   int32_t* seg;        // segment of the entry
   int32_t* miss;       // flat-het index or -1
   int32_t* seg_start;  // first entry of each segment, [nseg] = nvar
+  float* yt_prev;      // transition from the previous VAR site (0 for the first)
+  float* yt_next;      // transition to the next VAR site (0 for the last)
+  uint8_t* flags;      // bit0: first entry of its segment, bit1: last entry of its segment
   int32_t* nvar;
   int32_t* nseg;
   int32_t* nmiss;
@@ -39,8 +42,8 @@ void launch_build_vars(const int32_t* tsel, int nb, const int32_t* poly, const i
                        const uint8_t* h1, const uint8_t* flat, const uint8_t* lq, int L, PhaseVars V,
                        cudaStream_t s);
 int launch_phase(int J, const int32_t* tsel, int nb, const int32_t* nstates, const uint32_t* hvar, int WB, int Kp,
-                 const int32_t* poly, int L, const double* cm, PhaseVars V, PhaseStore S, const ModelConst& mc,
-                 uint64_t seed, int iteration, const int32_t* target_ids, cudaStream_t s);
+                 const int32_t* poly, const int32_t* npoly, int L, const double* cm, PhaseVars V, PhaseStore S,
+                 const ModelConst& mc, uint64_t seed, int iteration, const int32_t* target_ids, cudaStream_t s);
 void launch_phase_writeback(const int32_t* tsel, int nb, const int32_t* poly, const int32_t* polyidx, int L,
                             PhaseVars V, PhaseStore S, const ModelConst& mc, uint64_t seed, int iteration,
                             const int32_t* target_ids, uint8_t* h0, uint8_t* h1, cudaStream_t s);

@@ -229,10 +229,22 @@ def make_panel_and_targets(n_ref_haps, n_sites, region_mb, rare_frac, n_targets,
         hvar[ci, h // 8] ^= np.uint8(1 << (7 - h % 8))
         calt[s] += 1 if calt[s] == 0 else -1
     cref = N - calt
+    # common-generated sites whose minor count fell below the threshold get extra
+    # minor-allele copies so that they stay in HvarRef
+    need = int(math.ceil(sparse_maf * N))
+    for s in com_idx[np.minimum(cref[com_idx], calt[com_idx]) < need]:
+        ci = int(np.searchsorted(com_idx, s))
+        row = np.unpackbits(hvar[ci], count=N)
+        minor = 1 if calt[s] <= cref[s] else 0
+        cand = np.flatnonzero(row != minor)
+        add = rng.choice(cand, size=need - int(min(cref[s], calt[s])), replace=False)
+        row[add] = minor
+        hvar[ci] = np.packbits(row)[:stride]
+        calt[s] = int(row.sum())
+        cref[s] = N - calt[s]
     major = (calt > cref).astype(np.uint8)
     maf = np.minimum(cref, calt) / N
     flag_common = (maf >= sparse_maf).astype(np.uint8)
-    # sites generated as common must stay common so that HvarRef rows match
     if (flag_common[com_idx] == 0).any() or (flag_common[rare_idx] == 1).any():
         bad_c = com_idx[flag_common[com_idx] == 0]
         bad_r = rare_idx[flag_common[rare_idx] == 1]

@@ -84,6 +84,7 @@ def ref_lib():
                                      C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]
         lib.orc_std_sample.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int,
                                        C.POINTER(C.c_int32), C.POINTER(C.c_uint64)]
+        lib.orc_philox.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
         _ref = lib
     return _ref
 
@@ -296,3 +297,51 @@ def std_sample(seed, purpose, iteration, target, pop, n):
     used = C.c_uint64(0)
     k = ref_lib().orc_std_sample(seed, purpose, iteration, target, pop, n, _p(out, C.c_int32), C.byref(used))
     return out[:k].copy(), used.value
+
+
+def philox(ctr, key):
+    c = np.ascontiguousarray(ctr, np.uint32)
+    k = np.ascontiguousarray(key, np.uint32)
+    out = np.zeros(4, np.uint32)
+    ref_lib().orc_philox(_p(c, C.c_uint32), _p(k, C.c_uint32), _p(out, C.c_uint32))
+    return out
+
+
+def restate_lib():
+    global _restate
+    if _restate is None:
+        lib = C.CDLL(RESTATE_LIB)
+        lib.rs_impute.restype = C.c_double
+        lib.rs_impute.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_uint8), C.POINTER(C.c_uint8), C.POINTER(C.c_uint8),
+                                  C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_uint8), C.c_int,
+                                  C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_uint32), C.c_int,
+                                  C.c_double, C.c_float, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_uint8),
+                                  C.POINTER(C.c_float)]
+        _restate = lib
+    return _restate
+
+
+def restate_impute(panel, states, HL, flat, precision=64, ne=100000, err_imp=1e-12):
+    """FP64 (or FP32) restatement of imputation_hmm::computePosteriors; returns (HP, loglik)."""
+    lib = restate_lib()
+    L = panel.n_sites
+    comrow = np.full(L, -1, np.int32)
+    com = np.flatnonzero(panel.flag_common)
+    comrow[com] = np.arange(com.size, dtype=np.int32)
+    keep = [np.ascontiguousarray(x) for x in (panel.flag_common.astype(np.uint8), panel.lq.astype(np.uint8),
+                                              panel.major.astype(np.uint8), panel.cm.astype(np.float64), comrow,
+                                              panel.hvar.astype(np.uint8), panel.shap_off.astype(np.int64),
+                                              panel.shap_sites.astype(np.int32),
+                                              np.asarray(states, np.uint32), np.asarray(HL, np.float32),
+                                              np.asarray(flat, np.uint8))]
+    HP = np.zeros(2 * L, np.float32)
+    err = float(np.clip(np.float32(err_imp), np.float32(1e-12), np.float32(1e-3)))
+    ed = np.float32(err)
+    ee = np.float32(1.0 - float(ed))
+    nrho = (-0.04 * ne) / panel.n_ref_haps
+    ll = lib.rs_impute(precision, L, _p(keep[0], C.c_uint8), _p(keep[1], C.c_uint8), _p(keep[2], C.c_uint8),
+                       _p(keep[3], C.c_double), _p(keep[4], C.c_int32), _p(keep[5], C.c_uint8),
+                       (panel.n_ref_haps + 7) // 8, _p(keep[6], C.c_int64), _p(keep[7], C.c_int32),
+                       _p(keep[8], C.c_uint32), keep[8].size, nrho, float(ed), float(ee), _p(keep[9], C.c_float),
+                       _p(keep[10], C.c_uint8), _p(HP, C.c_float))
+    return HP, ll

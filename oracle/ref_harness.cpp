@@ -556,6 +556,11 @@ void orc_stream_words(uint64_t seed, uint32_t purpose, uint32_t iteration, uint3
   for (int i = 0; i < n; ++i) out[i] = gp::stream_word(seed, purpose, iteration, target, start + i);
 }
 
+// Raw Philox4x32-10 block, for known-answer tests of the stream generator.
+void orc_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+  gp::philox4x32_10(ctr[0], ctr[1], ctr[2], ctr[3], key[0], key[1], out);
+}
+
 // getFloat / getInt through the shimmed reference RNG class.
 void orc_rng_floats(uint64_t seed, uint32_t purpose, uint32_t iteration, uint32_t target, int n, float* out) {
   random_number_generator r;
