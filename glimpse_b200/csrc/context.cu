@@ -218,7 +218,7 @@ Context::~Context() {
   impute.states.release(); impute.nstates.release(); impute.states_off.release();
   impute.mark.release(); impute.polyidx.release(); impute.poly.release(); impute.npoly.release();
   impute.hvar.release(); impute.em.release(); impute.tr.release(); impute.fl.release();
-  impute.alpha.release(); impute.alpha_off.release();
+  impute.alpha.release(); impute.alpha_off.release(); impute.split.release(); impute.split_scr.release();
   impute.hl.release(); impute.hp.release(); impute.flat.release();
   prof_resolve();
   for (DevBuf* b : phase.all()) b->release();
@@ -285,22 +285,32 @@ int Context::run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
   if ((e = w.fl.ensure((size_t)n * L)) != cudaSuccess) return cuda_fail(e, "alloc fl");
   if ((e = w.alpha_off.ensure((size_t)n * 8)) != cudaSuccess) return cuda_fail(e, "alloc alpha_off");
   std::vector<int64_t> aoff(n);
+  std::vector<int32_t> split(n);
   int64_t tot = 0;
+  int Kmax = 0;
   for (int i = 0; i < n; ++i) {
     aoff[i] = tot;
     tot += (int64_t)impute_np[i] * w.Kp;
+    split[i] = (impute_np[i] / 2) & ~31;  // forward/backward meeting point, a multiple of 32
+    Kmax = std::max(Kmax, host_nstates[i]);
   }
   if ((e = w.alpha.ensure((size_t)std::max<int64_t>(tot, 1) * 4)) != cudaSuccess) return cuda_fail(e, "alloc alpha");
+  if ((e = w.split.ensure((size_t)n * 4)) != cudaSuccess) return cuda_fail(e, "alloc split");
+  if ((e = w.split_scr.ensure((size_t)n * (2 + w.Kp) * 4)) != cudaSuccess) return cuda_fail(e, "alloc split");
   cudaMemcpyAsync(w.alpha_off.ptr, aoff.data(), n * 8, cudaMemcpyHostToDevice, stream);
+  cudaMemcpyAsync(w.split.ptr, split.data(), n * 4, cudaMemcpyHostToDevice, stream);
   launch_site_records(panel, mc, w, d_hl, d_flat, stream);
   double cells = 0;
   for (int i = 0; i < n; ++i) cells += (double)impute_np[i] * (double)host_nstates[i];
+  // one warp per chain: lane-owned states in groups of 8 per lane
+  const int J = std::max(8, ((Kmax + 31) / 32 + 3 + 7) / 8 * 8);
   cudaEvent_t ea;
   prof_begin(ea);
-  launch_impute_fb(mc, w, d_hp, stream);
+  if (launch_impute_warp(1, J, mc, w, d_hp, stream) != GP_OK || launch_impute_warp(2, J, mc, w, d_hp, stream) != GP_OK)
+    return (fail(GP_E_ARG, "imputation: too many states"), GP_E_ARG);
   prof_end(ea, 0, cells);
   launch_impute_mono(panel, mc, w, d_hl, d_flat, d_hp, stream);
-  prof.kernel_launches += 3;
+  prof.kernel_launches += 4;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "imputation launch");
   return GP_OK;
 }

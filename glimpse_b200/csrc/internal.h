@@ -68,7 +68,7 @@ struct ImputeWork {
   DevBuf states, nstates, states_off;
   DevBuf mark, polyidx, poly, npoly;
   DevBuf hvar, em, tr, fl;
-  DevBuf alpha, alpha_off;
+  DevBuf alpha, alpha_off, split, split_scr;
   DevBuf hl, hp, flat;
 };
 
@@ -95,7 +95,7 @@ void launch_compact_poly(const DevPanel& P, ImputeWork& w, cudaStream_t s);
 void launch_build_hvar(const DevPanel& P, ImputeWork& w, cudaStream_t s);
 void launch_site_records(const DevPanel& P, const ModelConst& mc, ImputeWork& w, const float* hl,
                          const uint8_t* flat, cudaStream_t s);
-void launch_impute_fb(const ModelConst& mc, ImputeWork& w, float* hp, cudaStream_t s);
+int launch_impute_warp(int phase, int J, const ModelConst& mc, ImputeWork& w, float* hp, cudaStream_t s);
 void launch_impute_mono(const DevPanel& P, const ModelConst& mc, ImputeWork& w, const float* hl,
                         const uint8_t* flat, float* hp, cudaStream_t s);
 

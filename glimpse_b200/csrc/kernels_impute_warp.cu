@@ -1,0 +1,378 @@
+// Imputation HMM forward-backward with one warp per chain.
+//
+// The haploid Li-Stephens recursion (phase/src/models/imputation_hmm.cpp:143-416)
+// is sequential over sites with a sum over all K states at every site. Here a
+// single warp runs one chain: lane `lane` owns states k = lane + 32 j (j < J),
+// the per-site sums are warp butterflies (no block barrier), and all memory
+// traffic is streamed ahead of the chain:
+//   * Hvar words of the next 32-site block and the stored rows of the next D
+//     sites go through a per-warp shared-memory ring filled by cp.async;
+//   * per-site records (emissions, transitions, flags) of the next block are
+//     loaded by the lanes one block ahead.
+//
+// Each haplotype is split at M (a multiple of 32) into two chains that run
+// concurrently and meet in the middle (no waiting between them):
+//   phase 1  forward  [0, M)       stores alpha rows
+//            backward [np-1, M]    stores the pre-emission backward rows (prob_curr,
+//                                  1 at the last site) and leaves Beta at M
+//   phase 2  forward  [M, np)      alpha from row M-1; posteriors from alpha x prob_curr
+//            backward [M-1, 0]     Beta from site M; posteriors from stored alpha x prob_curr
+// Rows [0, M) of the store hold alpha and rows [M, np) prob_curr: one 4-byte
+// write and one read per (site, state), plus 1/8 byte of Hvar per pass.
+//
+// Sums follow a fixed order (lane-sequential over j, then a lane butterfly), so
+// results are deterministic. Every fused multiply-add is an explicit fmaf where
+// the reference's compiled arithmetic has one (build with --fmad=false).
+#include "internal.h"
+
+namespace gp {
+
+namespace {
+
+constexpr int kWarpsPerCta = 2;
+constexpr int kRowDepth = 3;              // stored rows fetched this many sites ahead
+constexpr int kRing = kRowDepth + 1;      // ring slots
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(smem)), "l"(gmem));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// Copy Kp 4-byte values (Kp a multiple of 32, 16-byte aligned) into shared memory.
+__device__ __forceinline__ void copy_row_async(void* dst, const void* src, int Kp, int lane) {
+  const int chunks = Kp >> 2;  // 16-byte chunks
+  const char* s = static_cast<const char*>(src);
+  char* d = static_cast<char*>(dst);
+  for (int c = lane; c < chunks; c += 32) cp_async16(d + 16 * c, s + 16 * c);
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = __fadd_rn(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+struct WarpScratch {
+  float* asum;          // [n] AlphaSum at site M-1
+  float* bsum;          // [n] betaSum at site M
+  float* brow;          // [n][Kp] Beta at site M
+  const int32_t* split; // [n] M
+};
+
+// Per-warp shared memory: records (2 blocks), Hvar words (2 blocks), row ring.
+struct WarpSmem {
+  float4* em;     // [2][32]
+  float2* tr;     // [2][32]
+  int32_t* pl;    // [2][32] site of the poly index
+  uint8_t* fl;    // [2][32]
+  uint32_t* words;  // [2][Kp]
+  float* ring;    // [kRing][Kp]
+};
+
+__device__ __forceinline__ WarpSmem carve(char* base, int Kp) {
+  WarpSmem m;
+  m.em = reinterpret_cast<float4*>(base);
+  m.tr = reinterpret_cast<float2*>(base + 2 * 32 * 16);
+  m.words = reinterpret_cast<uint32_t*>(base + 2 * 32 * 16 + 2 * 32 * 8);
+  m.ring = reinterpret_cast<float*>(base + 2 * 32 * 16 + 2 * 32 * 8 + 2 * (size_t)Kp * 4);
+  m.pl = reinterpret_cast<int32_t*>(base + 2 * 32 * 16 + 2 * 32 * 8 + 2 * (size_t)Kp * 4 +
+                                    (size_t)kRing * Kp * 4);
+  m.fl = reinterpret_cast<uint8_t*>(base + 2 * 32 * 16 + 2 * 32 * 8 + 2 * (size_t)Kp * 4 +
+                                    (size_t)kRing * Kp * 4 + 2 * 32 * 4);
+  return m;
+}
+
+__host__ __device__ __forceinline__ size_t warp_smem_bytes(int Kp) {
+  return 2 * 32 * 16 + 2 * 32 * 8 + 2 * (size_t)Kp * 4 + (size_t)kRing * Kp * 4 + 2 * 32 * 4 + 2 * 32 + 64;
+}
+
+__device__ __forceinline__ void write_posterior_w(float p0, float p1, uint8_t f, float4 e, const ModelConst& mc,
+                                                  float* hp_site) {
+  float po0, po1;
+  if (f) {
+    po0 = fmaf(p0, mc.ee_imp, __fmul_rn(p1, mc.ed_imp));
+    po1 = fmaf(p0, mc.ed_imp, __fmul_rn(p1, mc.ee_imp));
+    if (!(f & 1)) {
+      po0 = __fmul_rn(po0, e.z);
+      po1 = __fmul_rn(po1, e.w);
+    }
+  } else {
+    const float ph0 = p0 / e.x;
+    const float ph1 = p1 / e.y;
+    po0 = __fmul_rn(fmaf(ph0, mc.ee_imp, __fmul_rn(ph1, mc.ed_imp)), e.z);
+    po1 = __fmul_rn(fmaf(ph0, mc.ed_imp, __fmul_rn(ph1, mc.ee_imp)), e.w);
+  }
+  const float den = __fadd_rn(po0, po1);
+  hp_site[0] = po0 / den;
+  hp_site[1] = po1 / den;
+}
+
+// State layout inside a chain: the K states are padded to 32 * jn states with
+// jn a multiple of 4, and the padding is put in front: lane `lane` of group j
+// holds state k = 32 j + lane - pad (pad = 32 jn - K < 128). Only groups 0..3
+// contain padding, so only they carry validity masks; padded states are kept at
+// exactly 0 and therefore add nothing to any sum. Groups are processed in
+// chunks of 4 behind one warp-uniform branch, so a chain's work follows its own K.
+//
+// Site bits: the 32-bit Hvar word of a state covers a 32-site block; it is kept
+// shifted so that the current site's bit is the sign bit (bit-reversed for the
+// forward direction), which turns the emission choice into a sign test.
+template <int J>
+__global__ void __launch_bounds__(32 * kWarpsPerCta) k_impute_warp(
+    int phase, int nchains, const int32_t* __restrict__ poly, const int32_t* __restrict__ npoly,
+    const int32_t* __restrict__ nstates, const uint32_t* __restrict__ hvar, const float4* __restrict__ em,
+    const float2* __restrict__ tr, const uint8_t* __restrict__ fl, const int64_t* __restrict__ store_off,
+    float* __restrict__ store_pool, WarpScratch sc, int L, int WB, int Kp, ModelConst mc, float* __restrict__ hp) {
+  static_assert(J % 4 == 0, "groups are processed in chunks of 4");
+  extern __shared__ __align__(16) char smem_raw[];
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int chain = blockIdx.x * kWarpsPerCta + warp;
+  if (chain >= nchains) return;
+  const int t = chain >> 1;
+  const bool fwd = (chain & 1) == 0;
+  const int np = npoly[t];
+  const int K = nstates[t];
+  const int M = sc.split[t];
+  if (np == 0 || K == 0) return;
+  int lo, hi;
+  if (phase == 1) {
+    if (fwd) { lo = 0; hi = M; } else { lo = M; hi = np; }
+  } else {
+    if (fwd) { lo = M; hi = np; } else { lo = 0; hi = M; }
+  }
+  if (lo >= hi) return;
+  const int jn = (((K + 31) >> 5) + 3) & ~3;  // groups in use, a multiple of 4
+  const int pad = 32 * jn - K;
+  bool vg[4];                                 // validity of this lane in groups 0..3
+#pragma unroll
+  for (int j = 0; j < 4; ++j) vg[j] = (32 * j + lane) >= pad;
+  const int kb = lane - pad;                  // state index of group 0 for this lane
+  WarpSmem S = carve(smem_raw + (size_t)warp * warp_smem_bytes(Kp), Kp);
+  float* store = store_pool + store_off[t];
+  const uint32_t* hv = hvar + (size_t)t * WB * Kp;
+  const float4* E = em + (size_t)t * L;
+  const float2* T = tr + (size_t)t * L;
+  const uint8_t* F = fl + (size_t)t * L;
+  float* HP = hp + (size_t)t * 2 * L;
+  const int32_t* PL = poly + (size_t)t * L;
+  const bool post = (phase == 2);
+  const int n = hi - lo;
+  const float Kf = (float)K;
+  auto site_of = [&](int s) { return fwd ? lo + s : hi - 1 - s; };
+  auto block_of = [&](int s) { return site_of(s) >> 5; };
+  // index of the value owned by (j, lane) in a K-long row; padding reads entry 0
+  auto idx = [&](int j) { return max(32 * j + kb, 0); };
+
+  // ---- prologue ----
+  const int b_first = block_of(0);
+  const int b_last = block_of(n - 1);
+  const int dir = fwd ? 1 : -1;
+  {
+    const int l = (b_first << 5) + lane;
+    if (l < np) {
+      S.em[(b_first & 1) * 32 + lane] = E[l];
+      S.tr[(b_first & 1) * 32 + lane] = T[l];
+      S.fl[(b_first & 1) * 32 + lane] = F[l];
+      S.pl[(b_first & 1) * 32 + lane] = PL[l];
+    }
+    copy_row_async(S.words + (size_t)(b_first & 1) * Kp, hv + (size_t)b_first * Kp, Kp, lane);
+    if (b_first != b_last) {
+      const int b2 = b_first + dir;
+      copy_row_async(S.words + (size_t)(b2 & 1) * Kp, hv + (size_t)b2 * Kp, Kp, lane);
+    }
+  }
+  cp_commit();
+#pragma unroll
+  for (int d = 0; d < kRowDepth; ++d) {
+    if (post && d < n) copy_row_async(S.ring + (size_t)(d % kRing) * Kp, store + (size_t)site_of(d) * Kp, Kp, lane);
+    cp_commit();
+  }
+
+  float x[J];      // alpha (forward) or Beta (backward)
+  uint32_t w[J];   // Hvar bits, current site in the sign bit
+#pragma unroll
+  for (int j = 0; j < J; ++j) {
+    x[j] = 0.f;
+    w[j] = 0u;
+  }
+  float acc = 0.f;  // AlphaSum / betaSum of the previous step
+  float2 t_prev = make_float2(0.f, 0.f);
+  if (fwd && lo > 0) {
+#pragma unroll
+    for (int j = 0; j < J; ++j)
+      if (j < jn) x[j] = (j >= 4 || vg[j & 3]) ? store[(size_t)(lo - 1) * Kp + idx(j)] : 0.f;
+    acc = sc.asum[t];
+    t_prev = T[lo - 1];
+  }
+  if (!fwd && hi < np) {
+#pragma unroll
+    for (int j = 0; j < J; ++j)
+      if (j < jn) x[j] = (j >= 4 || vg[j & 3]) ? sc.brow[(size_t)t * Kp + idx(j)] : 0.f;
+    acc = sc.bsum[t];
+  }
+  float4 pe = make_float4(0.f, 0.f, 0.f, 0.f);
+  float2 pt = make_float2(0.f, 0.f);
+  uint8_t pf = 0;
+  int32_t pp = 0;
+  if (b_first != b_last) {
+    const int ln = ((b_first + dir) << 5) + lane;
+    if (ln < np) { pe = E[ln]; pt = T[ln]; pf = F[ln]; pp = PL[ln]; }
+  }
+  int cur_block = b_first;
+
+  for (int s = 0; s < n; ++s) {
+    const int l = site_of(s);
+    const int b = l >> 5;
+    const int i = l & 31;
+    const bool new_block = (s == 0) || (b != cur_block);
+    if (b != cur_block) {
+      S.em[(b & 1) * 32 + lane] = pe;
+      S.tr[(b & 1) * 32 + lane] = pt;
+      S.fl[(b & 1) * 32 + lane] = pf;
+      S.pl[(b & 1) * 32 + lane] = pp;
+      cur_block = b;
+      if (b != b_last) {
+        const int bn = b + dir;
+        const int ln = (bn << 5) + lane;
+        if (ln < np) { pe = E[ln]; pt = T[ln]; pf = F[ln]; pp = PL[ln]; }
+        copy_row_async(S.words + (size_t)(bn & 1) * Kp, hv + (size_t)bn * Kp, Kp, lane);
+      }
+    }
+    if (post && s + kRowDepth < n)
+      copy_row_async(S.ring + (size_t)((s + kRowDepth) % kRing) * Kp, store + (size_t)site_of(s + kRowDepth) * Kp,
+                     Kp, lane);
+    cp_commit();
+    cp_wait<kRowDepth>();
+    __syncwarp();
+    if (new_block) {
+      const uint32_t* wb = S.words + (size_t)(b & 1) * Kp;
+      // forward: site 0 of the block in the sign bit; backward: site i in the sign bit
+      const int sh = fwd ? i : 31 - i;
+#pragma unroll
+      for (int j = 0; j < J; ++j)
+        if (j < jn) {
+          const uint32_t v = wb[idx(j)];
+          w[j] = (fwd ? __brev(v) : v) << sh;
+        }
+    }
+    const uint8_t f = S.fl[(b & 1) * 32 + i];
+    const float4 e = S.em[(b & 1) * 32 + i];
+    const float* row = S.ring + (size_t)(s % kRing) * Kp;
+    float* srow = store + (size_t)l * Kp;
+    const bool last = (l == np - 1);
+    float q0[4] = {0.f, 0.f, 0.f, 0.f}, q1[4] = {0.f, 0.f, 0.f, 0.f}, q2[4] = {0.f, 0.f, 0.f, 0.f};
+    float fact1, fact2;
+    bool init;
+    if (fwd) {
+      init = (l == 0);
+      fact1 = init ? 1.0f / Kf : t_prev.x;  // t_prev.x = t / K of the previous site
+      fact2 = init ? 0.f : t_prev.y / acc;
+    } else {
+      init = last;
+      const float2 tt = S.tr[(b & 1) * 32 + i];
+      fact1 = init ? 1.0f / Kf : tt.x;
+      fact2 = init ? 0.f : tt.y / acc;
+    }
+    const bool emit = !f;
+#pragma unroll
+    for (int j0 = 0; j0 < J; j0 += 4) {
+      if (j0 < jn) {
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          const int j = j0 + jj;
+          const bool bit = (int32_t)w[j] < 0;
+          w[j] <<= 1;
+          // pre-emission value: forward x*f2+f1 (alpha), backward prob_curr;
+          // at the first (last) site: 1/K (imputation_hmm.cpp:155,187,262,339)
+          const float pcv = init ? fact1 : fmaf(x[j], fact2, fact1);
+          float nx = emit ? __fmul_rn(pcv, bit ? e.y : e.x) : pcv;
+          if (j < 4) nx = vg[jj] ? nx : 0.f;
+          x[j] = nx;
+          q0[jj] = __fadd_rn(q0[jj], nx);
+          const bool valid = (j >= 4) || vg[jj];
+          if (post) {
+            const float r = row[idx(j)];
+            // prob_hid terms: forward alpha x stored prob_curr (alpha alone at the
+            // last site), backward stored alpha x prob_curr (alpha alone at the last site)
+            float d = fwd ? (last ? nx : __fmul_rn(nx, r)) : (last ? r : __fmul_rn(r, pcv));
+            if (j < 4) d = valid ? d : 0.f;
+            q1[jj] = __fadd_rn(q1[jj], bit ? 0.f : d);
+            q2[jj] = __fadd_rn(q2[jj], bit ? d : 0.f);
+          } else if (valid) {
+            srow[idx(j)] = fwd ? nx : (last ? 1.0f : pcv);
+          }
+        }
+      }
+    }
+    const float v0 = warp_sum(__fadd_rn(__fadd_rn(q0[0], q0[1]), __fadd_rn(q0[2], q0[3])));
+    if (fwd) {
+      acc = (f && l == 0) ? 1.0f : v0;  // AlphaSum[0] = 1 at a flat first site (imputation_hmm.cpp:156)
+      t_prev = S.tr[(b & 1) * 32 + i];
+    } else {
+      acc = (f && last) ? 1.0f : v0;  // betaSum = 1 at a flat last site (imputation_hmm.cpp:285)
+    }
+    if (post) {
+      const float v1 = warp_sum(__fadd_rn(__fadd_rn(q1[0], q1[1]), __fadd_rn(q1[2], q1[3])));
+      const float v2 = warp_sum(__fadd_rn(__fadd_rn(q2[0], q2[1]), __fadd_rn(q2[2], q2[3])));
+      if (lane == 0) write_posterior_w(v1, v2, f, e, mc, HP + 2 * S.pl[(b & 1) * 32 + i]);
+    }
+    __syncwarp();
+  }
+  cp_wait<0>();
+  if (!post) {
+    if (fwd) {
+      if (lane == 0) sc.asum[t] = acc;
+    } else {
+#pragma unroll
+      for (int j = 0; j < J; ++j)
+        if (j < jn && (j >= 4 || vg[j & 3])) sc.brow[(size_t)t * Kp + idx(j)] = x[j];
+      if (lane == 0) sc.bsum[t] = acc;
+    }
+  }
+}
+
+}  // namespace
+
+size_t impute_warp_smem(int Kp) { return (size_t)kWarpsPerCta * warp_smem_bytes(Kp); }
+
+int launch_impute_warp(int phase, int J, const ModelConst& mc, ImputeWork& w, float* hp, cudaStream_t s) {
+  WarpScratch sc;
+  sc.asum = w.split_scr.as<float>();
+  sc.bsum = sc.asum + w.n;
+  sc.brow = sc.bsum + w.n;
+  sc.split = w.split.as<int32_t>();
+  const int nchains = 2 * w.n;
+  const dim3 g((nchains + kWarpsPerCta - 1) / kWarpsPerCta);
+  const size_t sm = impute_warp_smem(w.Kp);
+#define GP_WARP(JJ)                                                                                          \
+  case JJ: {                                                                                                 \
+    static bool attr = false;                                                                                \
+    if (!attr) {                                                                                             \
+      cudaFuncSetAttribute(k_impute_warp<JJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);      \
+      attr = true;                                                                                           \
+    }                                                                                                        \
+    k_impute_warp<JJ><<<g, 32 * kWarpsPerCta, sm, s>>>(phase, nchains, w.poly.as<int32_t>(),                 \
+                                                       w.npoly.as<int32_t>(), w.nstates.as<int32_t>(),       \
+                                                       w.hvar.as<uint32_t>(), w.em.as<float4>(),             \
+                                                       w.tr.as<float2>(), w.fl.as<uint8_t>(),                \
+                                                       w.alpha_off.as<int64_t>(), w.alpha.as<float>(), sc, w.L, \
+                                                       w.WB, w.Kp, mc, hp);                                  \
+    break;                                                                                                   \
+  }
+  switch (J) {
+    GP_WARP(8) GP_WARP(16) GP_WARP(24) GP_WARP(32) GP_WARP(40) GP_WARP(48) GP_WARP(56) GP_WARP(64)
+    default: return GP_E_ARG;
+  }
+#undef GP_WARP
+  return GP_OK;
+}
+
+}  // namespace gp

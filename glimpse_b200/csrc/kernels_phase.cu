@@ -178,12 +178,20 @@ __device__ __forceinline__ void block_sum8(float (&v)[8], float (*red)[NW][8], i
   const int warp = threadIdx.x >> 5;
   if ((lane & 3) == 0) red[buf][warp][((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1)] = c;
   __syncthreads();
+  // lane l combines warps for hypotheses (l >> 3) and (l >> 3) + 4; butterflies
+  // over the warp index (l & 7) give the lanes of a group identical totals
+  static_assert(NW == 8, "one lane per warp partial");
+  float x0 = red[buf][lane & 7][lane >> 3];
+  float x1 = red[buf][lane & 7][(lane >> 3) + 4];
 #pragma unroll
-  for (int h = 0; h < 8; ++h) {
-    float s = red[buf][0][h];
+  for (int o = 1; o < 8; o <<= 1) {
+    x0 = __fadd_rn(x0, __shfl_xor_sync(0xffffffffu, x0, o));
+    x1 = __fadd_rn(x1, __shfl_xor_sync(0xffffffffu, x1, o));
+  }
 #pragma unroll
-    for (int w = 1; w < NW; ++w) s = __fadd_rn(s, red[buf][w][h]);
-    out[h] = s;
+  for (int h = 0; h < 4; ++h) {
+    out[h] = __shfl_sync(0xffffffffu, x0, 8 * h);
+    out[h + 4] = __shfl_sync(0xffffffffu, x1, 8 * h);
   }
   buf ^= 1;
 }
@@ -345,7 +353,7 @@ struct WordCache {
 };
 
 template <int J>
-__global__ void __launch_bounds__(PT) k_phase(const int32_t* __restrict__ tsel, const int32_t* __restrict__ nstates,
+__global__ void __launch_bounds__(PT, 2) k_phase(const int32_t* __restrict__ tsel, const int32_t* __restrict__ nstates,
                                               const int32_t* __restrict__ npoly, const uint32_t* __restrict__ hvar,
                                               int WB, int Kp, int L, PhaseVars V, PhaseStore S, ModelConst mc,
                                               uint64_t seed, int iteration, const int32_t* __restrict__ target_ids) {
