@@ -114,6 +114,47 @@ __device__ __forceinline__ void write_posterior_w(float p0, float p1, uint8_t f,
   hp_site[1] = po1 / den;
 }
 
+// One site of a chain for the owned states, specialised at compile time:
+//   FWD   forward (alpha) or backward (Beta) recursion
+//   POST  phase 2: form prob_hid from the stored row instead of storing a row
+//   INIT  first forward / last backward site: the pre-emission value is 1/K
+// Flat or low-quality sites pass emissions (1, 1): the product by 1.0 is exact,
+// so the same loop serves both kinds of site.
+// At the last site the forward posterior uses alpha alone and the stored
+// prob_curr is 1 there, so alpha x 1 is used unchanged (imputation_hmm.cpp:337-368).
+template <int J, bool FWD, bool POST, bool INIT, class Idx>
+__device__ __forceinline__ void chain_step(float (&x)[J], uint32_t (&w)[J], float (&q0)[4], float (&q1)[4],
+                                           float (&q2)[4], const bool (&vg)[4], int jn, float fact1, float fact2,
+                                           float4 e, const float* row, float* srow, Idx idx) {
+#pragma unroll
+  for (int j0 = 0; j0 < J; j0 += 4) {
+    if (j0 < jn) {
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) {
+        const int j = j0 + jj;
+        const bool bit = (int32_t)w[j] < 0;
+        w[j] <<= 1;
+        const float pcv = INIT ? fact1 : fmaf(x[j], fact2, fact1);
+        float nx = __fmul_rn(pcv, bit ? e.y : e.x);
+        if (j < 4) nx = vg[jj] ? nx : 0.f;
+        x[j] = nx;
+        q0[jj] = __fadd_rn(q0[jj], nx);
+        if (POST) {
+          const float r = row[idx(j)];
+          float d;
+          if (FWD) d = __fmul_rn(nx, r);           // alpha x stored prob_curr (1 at the last site)
+          else d = INIT ? r : __fmul_rn(r, pcv);  // stored alpha x prob_curr; alpha alone at the last site
+          if (j < 4) d = vg[jj] ? d : 0.f;
+          q1[jj] = __fadd_rn(q1[jj], bit ? 0.f : d);
+          q2[jj] = __fadd_rn(q2[jj], bit ? d : 0.f);
+        } else if (j >= 4 || vg[jj]) {
+          srow[idx(j)] = FWD ? nx : (INIT ? 1.0f : pcv);
+        }
+      }
+    }
+  }
+}
+
 // State layout inside a chain: the K states are padded to 32 * jn states with
 // jn a multiple of 4, and the padding is put in front: lane `lane` of group j
 // holds state k = 32 j + lane - pad (pad = 32 jn - K < 128). Only groups 0..3
@@ -269,49 +310,27 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_impute_warp(
     float* srow = store + (size_t)l * Kp;
     const bool last = (l == np - 1);
     float q0[4] = {0.f, 0.f, 0.f, 0.f}, q1[4] = {0.f, 0.f, 0.f, 0.f}, q2[4] = {0.f, 0.f, 0.f, 0.f};
+    const bool init = fwd ? (l == 0) : last;
     float fact1, fact2;
-    bool init;
     if (fwd) {
-      init = (l == 0);
       fact1 = init ? 1.0f / Kf : t_prev.x;  // t_prev.x = t / K of the previous site
       fact2 = init ? 0.f : t_prev.y / acc;
     } else {
-      init = last;
       const float2 tt = S.tr[(b & 1) * 32 + i];
       fact1 = init ? 1.0f / Kf : tt.x;
       fact2 = init ? 0.f : tt.y / acc;
     }
-    const bool emit = !f;
-#pragma unroll
-    for (int j0 = 0; j0 < J; j0 += 4) {
-      if (j0 < jn) {
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj) {
-          const int j = j0 + jj;
-          const bool bit = (int32_t)w[j] < 0;
-          w[j] <<= 1;
-          // pre-emission value: forward x*f2+f1 (alpha), backward prob_curr;
-          // at the first (last) site: 1/K (imputation_hmm.cpp:155,187,262,339)
-          const float pcv = init ? fact1 : fmaf(x[j], fact2, fact1);
-          float nx = emit ? __fmul_rn(pcv, bit ? e.y : e.x) : pcv;
-          if (j < 4) nx = vg[jj] ? nx : 0.f;
-          x[j] = nx;
-          q0[jj] = __fadd_rn(q0[jj], nx);
-          const bool valid = (j >= 4) || vg[jj];
-          if (post) {
-            const float r = row[idx(j)];
-            // prob_hid terms: forward alpha x stored prob_curr (alpha alone at the
-            // last site), backward stored alpha x prob_curr (alpha alone at the last site)
-            float d = fwd ? (last ? nx : __fmul_rn(nx, r)) : (last ? r : __fmul_rn(r, pcv));
-            if (j < 4) d = valid ? d : 0.f;
-            q1[jj] = __fadd_rn(q1[jj], bit ? 0.f : d);
-            q2[jj] = __fadd_rn(q2[jj], bit ? d : 0.f);
-          } else if (valid) {
-            srow[idx(j)] = fwd ? nx : (last ? 1.0f : pcv);
-          }
-        }
-      }
+    // one specialised state loop per (direction, phase, first/last site)
+    const float4 ee = f ? make_float4(1.0f, 1.0f, e.z, e.w) : e;
+#define GP_STEP(FWD, POST, INIT) chain_step<J, FWD, POST, INIT>(x, w, q0, q1, q2, vg, jn, fact1, fact2, ee, row, srow, idx)
+    if (fwd) {
+      if (post) { if (init) GP_STEP(true, true, true); else GP_STEP(true, true, false); }
+      else { if (init) GP_STEP(true, false, true); else GP_STEP(true, false, false); }
+    } else {
+      if (post) { if (init) GP_STEP(false, true, true); else GP_STEP(false, true, false); }
+      else { if (init) GP_STEP(false, false, true); else GP_STEP(false, false, false); }
     }
+#undef GP_STEP
     const float v0 = warp_sum(__fadd_rn(__fadd_rn(q0[0], q0[1]), __fadd_rn(q0[2], q0[3])));
     if (fwd) {
       acc = (f && l == 0) ? 1.0f : v0;  // AlphaSum[0] = 1 at a flat first site (imputation_hmm.cpp:156)
