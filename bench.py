@@ -53,7 +53,7 @@ def load_peaks():
 
 def read_traffic_per_cell():
     """DRAM bytes per imputation cell from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "k_impute_fb_batched.md")
+    p = os.path.join(ROOT, "profiles", "k_impute_warp_batched.md")
     if not os.path.exists(p):
         return None
     with open(p) as f:
@@ -112,6 +112,25 @@ class ClockSampler:
         os.remove(self.path)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def rank_ops(dist, device):
+    """Barrier and max-over-ranks of a float (the step time) for the ranks of one job.
+    dist is torch.distributed with an initialised process group, or None for one rank."""
+    import torch
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    return barrier, max_over_ranks
 
 
 def cpu_sample(w, n_sample, threads, timed_iters=1):
@@ -184,16 +203,7 @@ def run_ours(args):
     ctx.set_targets(T, kpbwt=T.kpbwt)
     stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=torch.device("cuda", local))
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = rank_ops(dist, torch.device("cuda", local))
 
     def device_step():
         ctx.targets_reset()
@@ -257,7 +267,7 @@ def run_ours(args):
     achieved = prof["impute_bytes"] / (prof["impute_ms"] / 1000.0) / 1e9 if prof["impute_ms"] > 0 else 0.0
     per_launch_cells = prof["impute_cells"] / max(1, prof["impute_launches"])
     tpc = read_traffic_per_cell()
-    roofline = {"bound": "hbm", "kernel": "k_impute_fb (imputation forward-backward)", "achieved": achieved,
+    roofline = {"bound": "hbm", "kernel": "k_impute_warp (imputation forward-backward)", "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                 "algorithmic_bytes_per_cell": 8.25, "cells_per_launch": per_launch_cells,
                 "launch_ms": prof["impute_ms"] / max(1, prof["impute_launches"]),
