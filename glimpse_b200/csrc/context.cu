@@ -303,13 +303,13 @@ int Context::run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
   double cells = 0;
   for (int i = 0; i < n; ++i) cells += (double)impute_np[i] * (double)host_nstates[i];
   // one warp per chain: lane-owned states in groups of 8 per lane
-  const int J = std::max(8, ((Kmax + 31) / 32 + 3 + 7) / 8 * 8);
+  const int J = impute_groups(Kmax);
   cudaEvent_t ea;
   prof_begin(ea);
   if (launch_impute_warp(1, J, mc, w, d_hp, stream) != GP_OK || launch_impute_warp(2, J, mc, w, d_hp, stream) != GP_OK)
     return (fail(GP_E_ARG, "imputation: too many states"), GP_E_ARG);
   prof_end(ea, 0, cells);
-  launch_impute_mono(panel, mc, w, d_hl, d_flat, d_hp, stream);
+  launch_impute_finish(panel, mc, w, d_hl, d_flat, d_hp, stream);
   prof.kernel_launches += 4;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "imputation launch");
   return GP_OK;

@@ -96,7 +96,14 @@ void launch_build_hvar(const DevPanel& P, ImputeWork& w, cudaStream_t s);
 void launch_site_records(const DevPanel& P, const ModelConst& mc, ImputeWork& w, const float* hl,
                          const uint8_t* flat, cudaStream_t s);
 int launch_impute_warp(int phase, int J, const ModelConst& mc, ImputeWork& w, float* hp, cudaStream_t s);
-void launch_impute_mono(const DevPanel& P, const ModelConst& mc, ImputeWork& w, const float* hl,
+// Register groups per lane of the imputation chain for at most Kmax states: the
+// groups in use, ((K + 31) / 32 rounded up to a multiple of 4), rounded up to
+// the next instantiated size (8, 16, ..., 64).
+inline int impute_groups(int Kmax) {
+  const int jn = (((Kmax + 31) / 32) + 3) & ~3;
+  return jn <= 8 ? 8 : (jn + 7) / 8 * 8;
+}
+void launch_impute_finish(const DevPanel& P, const ModelConst& mc, ImputeWork& w, const float* hl,
                         const uint8_t* flat, float* hp, cudaStream_t s);
 
 }  // namespace gp

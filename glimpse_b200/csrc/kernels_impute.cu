@@ -173,13 +173,41 @@ __global__ void k_site_records(const int32_t* __restrict__ poly, const int32_t* 
   }
 }
 
-// Monomorphic sites take the major allele directly (imputation_hmm.cpp:417-429).
-__global__ void k_impute_mono(const int32_t* __restrict__ polyidx, const uint8_t* __restrict__ major,
-                              const float* __restrict__ hl, const uint8_t* __restrict__ flat, int L, ModelConst mc,
-                              float* __restrict__ hp) {
+// Posteriors of every site of a haplotype (imputation_hmm.cpp:337-368 and 417-429).
+// Poly sites: hp holds (prob_hid[0], prob_hid[1]) as the forward-backward left
+// it; the division by the emission, the mixing with the error rates and the HL
+// factor are applied here, off the sequential chain. Monomorphic sites take the
+// major allele directly.
+__global__ void k_impute_finish(const int32_t* __restrict__ polyidx, const uint8_t* __restrict__ major,
+                                const float4* __restrict__ em, const uint8_t* __restrict__ fl,
+                                const float* __restrict__ hl, const uint8_t* __restrict__ flat, int L, ModelConst mc,
+                                float* __restrict__ hp) {
   const int t = blockIdx.y;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < L; s += gridDim.x * blockDim.x) {
-    if (polyidx[(size_t)t * L + s] >= 0) continue;
+    const int pi = polyidx[(size_t)t * L + s];
+    float2* out = reinterpret_cast<float2*>(hp + (size_t)t * 2 * L + 2 * s);
+    if (pi >= 0) {
+      const float2 p = *out;
+      const float4 e = em[(size_t)t * L + pi];
+      const uint8_t f = fl[(size_t)t * L + pi];
+      float po0, po1;
+      if (f) {
+        po0 = fmaf(p.x, mc.ee_imp, __fmul_rn(p.y, mc.ed_imp));
+        po1 = fmaf(p.x, mc.ed_imp, __fmul_rn(p.y, mc.ee_imp));
+        if (!(f & 1)) {
+          po0 = __fmul_rn(po0, e.z);
+          po1 = __fmul_rn(po1, e.w);
+        }
+      } else {
+        const float ph0 = p.x / e.x;
+        const float ph1 = p.y / e.y;
+        po0 = __fmul_rn(fmaf(ph0, mc.ee_imp, __fmul_rn(ph1, mc.ed_imp)), e.z);
+        po1 = __fmul_rn(fmaf(ph0, mc.ed_imp, __fmul_rn(ph1, mc.ee_imp)), e.w);
+      }
+      const float den = __fadd_rn(po0, po1);
+      *out = make_float2(po0 / den, po1 / den);
+      continue;
+    }
     float p0 = major[s] ? mc.ed_imp : mc.ee_imp;
     float p1 = major[s] ? mc.ee_imp : mc.ed_imp;
     if (!flat[(size_t)t * L + s]) {
@@ -187,8 +215,7 @@ __global__ void k_impute_mono(const int32_t* __restrict__ polyidx, const uint8_t
       p1 = __fmul_rn(p1, hl[(size_t)t * 2 * L + 2 * s + 1]);
     }
     const float den = __fadd_rn(p0, p1);
-    hp[(size_t)t * 2 * L + 2 * s] = p0 / den;
-    hp[(size_t)t * 2 * L + 2 * s + 1] = p1 / den;
+    *out = make_float2(p0 / den, p1 / den);
   }
 }
 
@@ -230,10 +257,11 @@ void launch_site_records(const DevPanel& P, const ModelConst& mc, ImputeWork& w,
                                    w.em.as<float4>(), w.tr.as<float2>(), w.fl.as<uint8_t>());
 }
 
-void launch_impute_mono(const DevPanel& P, const ModelConst& mc, ImputeWork& w, const float* hl,
-                        const uint8_t* flat, float* hp, cudaStream_t s) {
+void launch_impute_finish(const DevPanel& P, const ModelConst& mc, ImputeWork& w, const float* hl,
+                          const uint8_t* flat, float* hp, cudaStream_t s) {
   dim3 g(grid_for(P.L, 256, 512), w.n);
-  k_impute_mono<<<g, 256, 0, s>>>(w.polyidx.as<int32_t>(), P.major, hl, flat, P.L, mc, hp);
+  k_impute_finish<<<g, 256, 0, s>>>(w.polyidx.as<int32_t>(), P.major, w.em.as<float4>(), w.fl.as<uint8_t>(), hl, flat,
+                                    P.L, mc, hp);
 }
 
 }  // namespace gp

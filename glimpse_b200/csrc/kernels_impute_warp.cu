@@ -45,12 +45,16 @@ __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-// Copy Kp 4-byte values (Kp a multiple of 32, 16-byte aligned) into shared memory.
+// Copy Kp 4-byte values (Kp a multiple of 32, at most 32 * J, 16-byte aligned)
+// into shared memory: 16-byte chunk lane + 32 c for c < J / 4.
+template <int J>
 __device__ __forceinline__ void copy_row_async(void* dst, const void* src, int Kp, int lane) {
-  const int chunks = Kp >> 2;  // 16-byte chunks
-  const char* s = static_cast<const char*>(src);
-  char* d = static_cast<char*>(dst);
-  for (int c = lane; c < chunks; c += 32) cp_async16(d + 16 * c, s + 16 * c);
+  const int chunks = Kp >> 2;
+  const char* s = static_cast<const char*>(src) + 16 * lane;
+  char* d = static_cast<char*>(dst) + 16 * lane;
+#pragma unroll
+  for (int c = 0; c < J / 4; ++c)
+    if (lane + 32 * c < chunks) cp_async16(d + 512 * c, s + 512 * c);
 }
 
 __device__ __forceinline__ float warp_sum(float v) {
@@ -93,27 +97,6 @@ __host__ __device__ __forceinline__ size_t warp_smem_bytes(int Kp) {
   return 2 * 32 * 16 + 2 * 32 * 8 + 2 * (size_t)Kp * 4 + (size_t)kRing * Kp * 4 + 2 * 32 * 4 + 2 * 32 + 64;
 }
 
-__device__ __forceinline__ void write_posterior_w(float p0, float p1, uint8_t f, float4 e, const ModelConst& mc,
-                                                  float* hp_site) {
-  float po0, po1;
-  if (f) {
-    po0 = fmaf(p0, mc.ee_imp, __fmul_rn(p1, mc.ed_imp));
-    po1 = fmaf(p0, mc.ed_imp, __fmul_rn(p1, mc.ee_imp));
-    if (!(f & 1)) {
-      po0 = __fmul_rn(po0, e.z);
-      po1 = __fmul_rn(po1, e.w);
-    }
-  } else {
-    const float ph0 = p0 / e.x;
-    const float ph1 = p1 / e.y;
-    po0 = __fmul_rn(fmaf(ph0, mc.ee_imp, __fmul_rn(ph1, mc.ed_imp)), e.z);
-    po1 = __fmul_rn(fmaf(ph0, mc.ed_imp, __fmul_rn(ph1, mc.ee_imp)), e.w);
-  }
-  const float den = __fadd_rn(po0, po1);
-  hp_site[0] = po0 / den;
-  hp_site[1] = po1 / den;
-}
-
 // One site of a chain for the owned states, specialised at compile time:
 //   FWD   forward (alpha) or backward (Beta) recursion
 //   POST  phase 2: form prob_hid from the stored row instead of storing a row
@@ -122,33 +105,37 @@ __device__ __forceinline__ void write_posterior_w(float p0, float p1, uint8_t f,
 // so the same loop serves both kinds of site.
 // At the last site the forward posterior uses alpha alone and the stored
 // prob_curr is 1 there, so alpha x 1 is used unchanged (imputation_hmm.cpp:337-368).
-template <int J, bool FWD, bool POST, bool INIT, class Idx>
-__device__ __forceinline__ void chain_step(float (&x)[J], uint32_t (&w)[J], float (&q0)[4], float (&q1)[4],
-                                           float (&q2)[4], const bool (&vg)[4], int jn, float fact1, float fact2,
-                                           float4 e, const float* row, float* srow, Idx idx) {
+// m selects the current site's bit in the Hvar words; rowl / srowl point at this
+// lane's state of group 0 in the staged row (shared) and in the stored row
+// (global), so group j is at offset 32 j. Padded lanes of groups 0..3 never
+// dereference them.
+template <int J, bool FWD, bool POST, bool INIT>
+__device__ __forceinline__ void chain_step(float (&x)[J], const uint32_t (&w)[J], uint32_t m, float (&q0)[4],
+                                           float (&q1)[4], float (&q2)[4], const bool (&vg)[4], int jn, float fact1,
+                                           float fact2, float ex, float ey, const float* rowl, float* srowl) {
 #pragma unroll
   for (int j0 = 0; j0 < J; j0 += 4) {
     if (j0 < jn) {
 #pragma unroll
       for (int jj = 0; jj < 4; ++jj) {
         const int j = j0 + jj;
-        const bool bit = (int32_t)w[j] < 0;
-        w[j] <<= 1;
+        const bool valid = j >= 4 || vg[jj];
+        const bool bit = (w[j] & m) != 0u;
         const float pcv = INIT ? fact1 : fmaf(x[j], fact2, fact1);
-        float nx = __fmul_rn(pcv, bit ? e.y : e.x);
-        if (j < 4) nx = vg[jj] ? nx : 0.f;
+        float nx = __fmul_rn(pcv, bit ? ey : ex);
+        if (j < 4) nx = valid ? nx : 0.f;
         x[j] = nx;
         q0[jj] = __fadd_rn(q0[jj], nx);
         if (POST) {
-          const float r = row[idx(j)];
+          float r = 0.f;
+          if (valid) r = rowl[32 * j];
           float d;
           if (FWD) d = __fmul_rn(nx, r);           // alpha x stored prob_curr (1 at the last site)
           else d = INIT ? r : __fmul_rn(r, pcv);  // stored alpha x prob_curr; alpha alone at the last site
-          if (j < 4) d = vg[jj] ? d : 0.f;
-          q1[jj] = __fadd_rn(q1[jj], bit ? 0.f : d);
-          q2[jj] = __fadd_rn(q2[jj], bit ? d : 0.f);
-        } else if (j >= 4 || vg[jj]) {
-          srow[idx(j)] = FWD ? nx : (INIT ? 1.0f : pcv);
+          if (bit) q2[jj] = __fadd_rn(q2[jj], d);
+          else q1[jj] = __fadd_rn(q1[jj], d);
+        } else if (valid) {
+          srowl[32 * j] = FWD ? nx : (INIT ? 1.0f : pcv);
         }
       }
     }
@@ -224,16 +211,16 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_impute_warp(
       S.fl[(b_first & 1) * 32 + lane] = F[l];
       S.pl[(b_first & 1) * 32 + lane] = PL[l];
     }
-    copy_row_async(S.words + (size_t)(b_first & 1) * Kp, hv + (size_t)b_first * Kp, Kp, lane);
+    copy_row_async<J>(S.words + (size_t)(b_first & 1) * Kp, hv + (size_t)b_first * Kp, Kp, lane);
     if (b_first != b_last) {
       const int b2 = b_first + dir;
-      copy_row_async(S.words + (size_t)(b2 & 1) * Kp, hv + (size_t)b2 * Kp, Kp, lane);
+      copy_row_async<J>(S.words + (size_t)(b2 & 1) * Kp, hv + (size_t)b2 * Kp, Kp, lane);
     }
   }
   cp_commit();
 #pragma unroll
   for (int d = 0; d < kRowDepth; ++d) {
-    if (post && d < n) copy_row_async(S.ring + (size_t)(d % kRing) * Kp, store + (size_t)site_of(d) * Kp, Kp, lane);
+    if (post && d < n) copy_row_async<J>(S.ring + (size_t)(d % kRing) * Kp, store + (size_t)site_of(d) * Kp, Kp, lane);
     cp_commit();
   }
 
@@ -284,30 +271,26 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_impute_warp(
         const int bn = b + dir;
         const int ln = (bn << 5) + lane;
         if (ln < np) { pe = E[ln]; pt = T[ln]; pf = F[ln]; pp = PL[ln]; }
-        copy_row_async(S.words + (size_t)(bn & 1) * Kp, hv + (size_t)bn * Kp, Kp, lane);
+        copy_row_async<J>(S.words + (size_t)(bn & 1) * Kp, hv + (size_t)bn * Kp, Kp, lane);
       }
     }
     if (post && s + kRowDepth < n)
-      copy_row_async(S.ring + (size_t)((s + kRowDepth) % kRing) * Kp, store + (size_t)site_of(s + kRowDepth) * Kp,
+      copy_row_async<J>(S.ring + (size_t)((s + kRowDepth) % kRing) * Kp, store + (size_t)site_of(s + kRowDepth) * Kp,
                      Kp, lane);
     cp_commit();
     cp_wait<kRowDepth>();
     __syncwarp();
     if (new_block) {
-      const uint32_t* wb = S.words + (size_t)(b & 1) * Kp;
-      // forward: site 0 of the block in the sign bit; backward: site i in the sign bit
-      const int sh = fwd ? i : 31 - i;
+      const uint32_t* wbl = S.words + (size_t)(b & 1) * Kp + kb;
 #pragma unroll
       for (int j = 0; j < J; ++j)
-        if (j < jn) {
-          const uint32_t v = wb[idx(j)];
-          w[j] = (fwd ? __brev(v) : v) << sh;
-        }
+        if (j < jn) w[j] = (j >= 4 || vg[j & 3]) ? wbl[32 * j] : 0u;
     }
+    const uint32_t m = 1u << i;
     const uint8_t f = S.fl[(b & 1) * 32 + i];
     const float4 e = S.em[(b & 1) * 32 + i];
-    const float* row = S.ring + (size_t)(s % kRing) * Kp;
-    float* srow = store + (size_t)l * Kp;
+    const float* rowl = S.ring + (size_t)(s % kRing) * Kp + kb;
+    float* srowl = store + (size_t)l * Kp + kb;
     const bool last = (l == np - 1);
     float q0[4] = {0.f, 0.f, 0.f, 0.f}, q1[4] = {0.f, 0.f, 0.f, 0.f}, q2[4] = {0.f, 0.f, 0.f, 0.f};
     const bool init = fwd ? (l == 0) : last;
@@ -321,8 +304,9 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_impute_warp(
       fact2 = init ? 0.f : tt.y / acc;
     }
     // one specialised state loop per (direction, phase, first/last site)
-    const float4 ee = f ? make_float4(1.0f, 1.0f, e.z, e.w) : e;
-#define GP_STEP(FWD, POST, INIT) chain_step<J, FWD, POST, INIT>(x, w, q0, q1, q2, vg, jn, fact1, fact2, ee, row, srow, idx)
+    const float ex = f ? 1.0f : e.x, ey = f ? 1.0f : e.y;
+#define GP_STEP(FWD, POST, INIT) \
+  chain_step<J, FWD, POST, INIT>(x, w, m, q0, q1, q2, vg, jn, fact1, fact2, ex, ey, rowl, srowl)
     if (fwd) {
       if (post) { if (init) GP_STEP(true, true, true); else GP_STEP(true, true, false); }
       else { if (init) GP_STEP(true, false, true); else GP_STEP(true, false, false); }
@@ -341,7 +325,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_impute_warp(
     if (post) {
       const float v1 = warp_sum(__fadd_rn(__fadd_rn(q1[0], q1[1]), __fadd_rn(q1[2], q1[3])));
       const float v2 = warp_sum(__fadd_rn(__fadd_rn(q2[0], q2[1]), __fadd_rn(q2[2], q2[3])));
-      if (lane == 0) write_posterior_w(v1, v2, f, e, mc, HP + 2 * S.pl[(b & 1) * 32 + i]);
+      // prob_hid of the two alleles; k_impute_finish turns them into HP
+      if (lane == 0) *reinterpret_cast<float2*>(HP + 2 * S.pl[(b & 1) * 32 + i]) = make_float2(v1, v2);
     }
     __syncwarp();
   }
