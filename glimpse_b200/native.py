@@ -22,6 +22,7 @@ EXPORTS = [
     "gp_run", "gp_haps_get", "gp_haps_set", "gp_posteriors_get", "gp_states_get", "gp_finalize", "gp_gp_get",
     "gp_impute_batch", "gp_rephase_batch", "gp_select", "gp_pbwt_states_get", "gp_sparse_pbwt_get",
     "gp_stage_times", "gp_build_sparse_pbwt", "gp_profile_get", "gp_profile_reset", "gp_stream",
+    "gp_impute_one_static",
     "gp_targets_reset",
 ]
 
@@ -171,6 +172,16 @@ class Context:
         hp = np.zeros((n, 2 * self.L), np.float32)
         self._check(self.lib.gp_impute_batch(self.h, n, _p(off, C.c_int64), _p(st, C.c_uint32), _p(hl, C.c_float),
                                              _p(flat, C.c_uint8), _p(hp, C.c_float)))
+        return hp
+
+    def impute_one_static(self, states, hl, flat):
+        """gp_impute_one_static: one haplotype, scratch in the library's fixed device region."""
+        st = np.ascontiguousarray(states, np.uint32)
+        hl = np.ascontiguousarray(hl, np.float32).reshape(2 * self.L)
+        flat = np.ascontiguousarray(flat, np.uint8).reshape(self.L)
+        hp = np.zeros(2 * self.L, np.float32)
+        self._check(self.lib.gp_impute_one_static(self.h, st.size, _p(st, C.c_uint32), _p(hl, C.c_float),
+                                                  _p(flat, C.c_uint8), _p(hp, C.c_float)))
         return hp
 
     def rephase_batch(self, states_list, h0, h1, flat, iteration, target_ids=None):

@@ -133,6 +133,16 @@ int gp_gp_get(gp_ctx* ctx, float* gp0, float* gp1, float* ds, uint8_t* gt0, uint
 int gp_impute_batch(gp_ctx* ctx, int32_t n, const int64_t* states_off, const uint32_t* states, const float* hl,
                     const uint8_t* flat, float* hp);
 
+/* No counterpart in the reference. The same computation as gp_impute_batch
+ * with n = 1 (k sorted state ids; hl, hp: 2L floats; flat: L bytes), for
+ * callers that must not allocate device memory during the call: all scratch
+ * lives in one fixed 64 MiB region per device inside the library. Calls whose
+ * scratch (about n_sites x k x 4 bytes, plus per-site records) would exceed it
+ * return GP_E_ARG. The first call on a device looks the region up and should
+ * come before any stream capture. Overlapping calls on one device race. */
+int gp_impute_one_static(gp_ctx* ctx, int32_t k, const uint32_t* states, const float* hl, const uint8_t* flat,
+                         float* hp);
+
 /* phasing_hmm::rephaseHaplotypes(H0, H1, flat) (phasing_hmm.h:136) for n
  * diploid targets with explicit conditioning sets; h0/h1 updated in place
  * (n x L). Target t draws from stream (RNG_PHASE, iteration, target_ids[t]). */
