@@ -6,6 +6,8 @@
 // hypothesis sums (probSumH) are block reductions; SUMK is per state.
 // Segment-start messages (phasingProb) and flat-het messages (imputeProb) from
 // the backward pass are stored in global memory as [seg][k][8] rows.
+#include <cstddef>
+
 #include <cub/block/block_scan.cuh>
 
 #include "internal.h"
@@ -215,6 +217,8 @@ __device__ __forceinline__ float transition(const double* __restrict__ cm, int p
 }
 
 struct PhaseShared {
+  // per VAR code: emissions of the 8 hypotheses for a state allele of 0 ([0..7]) and 1 ([8..15]); read as float4
+  __align__(16) float etab[16][16];
   float red[2][NW][8];
   float sumH[8];
   float sumT;
@@ -223,66 +227,101 @@ struct PhaseShared {
   int dip;
   int err;
 };
+static_assert(alignof(PhaseShared) >= 16 && offsetof(PhaseShared, etab) % 16 == 0, "etab rows are read as float4");
 
-// One site update: INIT / RUN / COLLAPSE of PEAK_HET, PEAK_HOM or FLAT_HET
-// (phasing_hmm.h:140-366), then the hypothesis sums.
-template <int J>
+// Emission table of the VAR codes (phasing_hmm.h:140-366): a peak het of type
+// typ emits ee where the state allele equals the hypothesis allele and ed
+// elsewhere; a peak hom emits 1 for the observed allele and ed/ee for the other;
+// a flat het emits nothing (1). Entries of unused codes are 1.
+__device__ __forceinline__ void fill_emission_table(float (*etab)[16], const ModelConst& mc, int tid) {
+  if (tid < 16 * 16) {
+    const int code = tid >> 4, a = (tid >> 3) & 1, h = tid & 7;
+    const int typ = code & 7, alt = (code >> 3) & 1;
+    const float mism = mc.ed_phs / mc.ee_phs;
+    float e = 1.0f;
+    if (typ < 3) e = (a == hyp_allele(h, typ)) ? mc.ee_phs : mc.ed_phs;
+    else if (typ == VT_HOM) e = (a != alt) ? mism : 1.0f;
+    etab[code][a * 8 + h] = e;
+  }
+}
+
+// One site update: INIT / RUN / COLLAPSE (phasing_hmm.h:140-366) for every VAR
+// type at once: the type enters only through the emission vectors e0 / e1 (state
+// allele 0 / 1), and a factor of exactly 1 leaves a product unchanged, so peak
+// hets, peak homs and flat hets share one loop. m selects the site's bit in the
+// Hvar words. Ends with the hypothesis sums.
+template <int J, int MODE>
 __device__ __forceinline__ void site_update(float (&prob)[J][8], const float (&sumk)[J], const uint32_t (&w)[J],
-                                            int sh, int K, int tid, int typ, int alt, int mode, float yt, float nt,
-                                            const ModelConst& mc, float (&sumH)[8], float& sumT,
-                                            float (*red)[NW][8], int& buf) {
-  // mode: 0 INIT, 1 RUN, 2 COLLAPSE
-  const float Kf = (float)K;
+                                            uint32_t m, int K, int tid, const float (&e0)[8], const float (&e1)[8],
+                                            float yt, float nt, float (&sumH)[8], float& sumT, float (*red)[NW][8],
+                                            int& buf) {
   float tF[8];
   float ntp = 0.f;
-  if (mode != 0) {
-    const float sc = yt / __fmul_rn(Kf, sumT);
+  if (MODE != 0) {
+    const float sc = yt / __fmul_rn((float)K, sumT);
 #pragma unroll
     for (int h = 0; h < 8; ++h) tF[h] = __fmul_rn(sumH[h], sc);
     ntp = nt / sumT;
   }
-  const float mism = mc.ed_phs / mc.ee_phs;
   float part[8];
 #pragma unroll
   for (int h = 0; h < 8; ++h) part[h] = 0.f;
-  if (typ == VT_FLAT && mode == 0) {
-    const float v = 1.0f / (float)(8u * (unsigned)K);
-#pragma unroll
-    for (int j = 0; j < J; ++j)
-#pragma unroll
-      for (int h = 0; h < 8; ++h) prob[j][h] = v;
-#pragma unroll
-    for (int h = 0; h < 8; ++h) sumH[h] = 0.125f;
-    sumT = 1.0f;
-    return;
-  }
 #pragma unroll
   for (int j = 0; j < J; ++j) {
     const int k = tid + j * PT;
     if (k >= K) continue;
-    const int bit = (w[j] >> sh) & 1u;
+    const bool bit = (w[j] & m) != 0u;
 #pragma unroll
     for (int h = 0; h < 8; ++h) {
-      float base;
-      if (mode == 0) base = 1.0f;
-      else if (mode == 1) base = fmaf(prob[j][h], ntp, tF[h]);
-      else base = fmaf(sumk[j], ntp, tF[h]);
+      const float e = bit ? e1[h] : e0[h];
       float v;
-      if (typ < 3) {
-        const float e = (bit == hyp_allele(h, typ)) ? mc.ee_phs : mc.ed_phs;
-        v = (mode == 0) ? e : __fmul_rn(base, e);
-      } else if (typ == VT_HOM) {
-        if (mode == 0) v = (bit != alt) ? mism : 1.0f;
-        else v = (bit != alt) ? __fmul_rn(base, mism) : base;
-      } else {
-        v = base;  // flat het: no emission
-      }
+      if (MODE == 0) v = e;
+      else if (MODE == 1) v = __fmul_rn(fmaf(prob[j][h], ntp, tF[h]), e);
+      else v = __fmul_rn(fmaf(sumk[j], ntp, tF[h]), e);
       prob[j][h] = v;
       part[h] = __fadd_rn(part[h], v);
     }
   }
   block_sum8(part, red, buf, sumH);
   sumT = hadd8(sumH);
+}
+
+// INIT at a flat het: every message is 1 / (8 K) (phasing_hmm.h:140-366).
+template <int J>
+__device__ __forceinline__ void site_init_flat(float (&prob)[J][8], int K, float (&sumH)[8], float& sumT) {
+  const float v = 1.0f / (float)(8u * (unsigned)K);
+#pragma unroll
+  for (int j = 0; j < J; ++j)
+#pragma unroll
+    for (int h = 0; h < 8; ++h) prob[j][h] = v;
+#pragma unroll
+  for (int h = 0; h < 8; ++h) sumH[h] = 0.125f;
+  sumT = 1.0f;
+}
+
+// Emission vectors of a VAR code from the shared table.
+__device__ __forceinline__ void load_emissions(const float (*etab)[16], int code, float (&e0)[8], float (&e1)[8]) {
+  const float4* r = reinterpret_cast<const float4*>(etab[code]);
+  const float4 a = r[0], b = r[1], c = r[2], d = r[3];
+  e0[0] = a.x; e0[1] = a.y; e0[2] = a.z; e0[3] = a.w; e0[4] = b.x; e0[5] = b.y; e0[6] = b.z; e0[7] = b.w;
+  e1[0] = c.x; e1[1] = c.y; e1[2] = c.z; e1[3] = c.w; e1[4] = d.x; e1[5] = d.y; e1[6] = d.z; e1[7] = d.w;
+}
+
+// One VAR site with the mode chosen at run time (warp-uniform).
+template <int J>
+__device__ __forceinline__ void site_step(int mode, int code, float (&prob)[J][8], const float (&sumk)[J],
+                                          const uint32_t (&w)[J], uint32_t m, int K, int tid,
+                                          const float (*etab)[16], float yt, float nt, float (&sumH)[8],
+                                          float& sumT, float (*red)[NW][8], int& buf) {
+  if (mode == 0 && (code & 7) == VT_FLAT) {
+    site_init_flat<J>(prob, K, sumH, sumT);
+    return;
+  }
+  float e0[8], e1[8];
+  load_emissions(etab, code, e0, e1);
+  if (mode == 1) site_update<J, 1>(prob, sumk, w, m, K, tid, e0, e1, yt, nt, sumH, sumT, red, buf);
+  else if (mode == 2) site_update<J, 2>(prob, sumk, w, m, K, tid, e0, e1, yt, nt, sumH, sumT, red, buf);
+  else site_update<J, 0>(prob, sumk, w, m, K, tid, e0, e1, yt, nt, sumH, sumT, red, buf);
 }
 
 // VAR records of 32 consecutive entries, double-buffered in shared memory.
@@ -367,6 +406,7 @@ __global__ void __launch_bounds__(PT, 2) k_phase(const int32_t* __restrict__ tse
   const int tid = threadIdx.x;
   const bool loader = tid < 32;
   if (tid == 0) sm.err = 0;
+  fill_emission_table(sm.etab, mc, tid);  // read after the first barrier below
   const uint32_t* hv = hvar + (size_t)t * WB * Kp;
   const int nblk_poly = (npoly[t] + 31) >> 5;
   const size_t vbase = (size_t)b * L;
@@ -421,13 +461,13 @@ __global__ void __launch_bounds__(PT, 2) k_phase(const int32_t* __restrict__ tse
       const int l = vs.l[cur][ii];
       wc.need(l >> 5, -1, hv, nblk_poly, Kp, K, tid);
       const int code = vs.code[cur][ii];
-      const int typ = code & 7, alt = (code >> 3) & 1;
+      const int typ = code & 7;
       const int seg = vs.seg[cur][ii];
       const int fl = vs.flags[cur][ii];
       const float yt = vs.ytn[cur][ii];
       const float nt = 1.0f - yt;
       const int mode = (i == nv - 1) ? 0 : ((fl & 2) ? 2 : 1);
-      site_update<J>(prob, sumk, wc.w, l & 31, K, tid, typ, alt, mode, yt, nt, mc, sumH, sumT, sm.red, buf);
+      site_step<J>(mode, code, prob, sumk, wc.w, 1u << (l & 31), K, tid, sm.etab, yt, nt, sumH, sumT, sm.red, buf);
       if (fl & 1) {
         do_sumk();
         store_rows(PP + (size_t)seg * K * 8);
@@ -483,13 +523,13 @@ __global__ void __launch_bounds__(PT, 2) k_phase(const int32_t* __restrict__ tse
       const int l = vs.l[cur][ii];
       wc.need(l >> 5, 1, hv, nblk_poly, Kp, K, tid);
       const int code = vs.code[cur][ii];
-      const int typ = code & 7, alt = (code >> 3) & 1;
+      const int typ = code & 7;
       const int seg = vs.seg[cur][ii];
       const int fl = vs.flags[cur][ii];
       const float yt = vs.ytp[cur][ii];
       const float nt = 1.0f - yt;
       const int mode = (i == 0) ? 0 : ((fl & 1) ? 2 : 1);
-      site_update<J>(prob, sumk, wc.w, l & 31, K, tid, typ, alt, mode, yt, nt, mc, sumH, sumT, sm.red, buf);
+      site_step<J>(mode, code, prob, sumk, wc.w, 1u << (l & 31), K, tid, sm.etab, yt, nt, sumH, sumT, sm.red, buf);
       const bool seg_end = (fl & 2) != 0;
       if (seg_end) do_sumk();
       if (seg_end && i != nv - 1) {
