@@ -103,6 +103,37 @@ __global__ void k_pbwt_rng(PbwtSelectArgs a) {
   for (int e = 0; e < a.n_haps; ++e) a.start_idx[e] = (int32_t)uniform_uint(g, 0u, (uint32_t)(a.N - 1));
 }
 
+// Per target haplotype, the non-LQ rare sites where it carries the non-major
+// allele, as bits: what the init_rare scan of haplotype_set.cpp:655-680 looks
+// for, so that the sweep can test a whole run of rare sites at once.
+__global__ void k_rare_carriers(PbwtSelectArgs a) {
+  const int hp = blockIdx.y;
+  const int t = a.hap_target[hp];
+  const uint8_t* H = (a.hap_which[hp] ? a.h1 : a.h0) + (size_t)t * a.L;
+  for (int wi = blockIdx.x * blockDim.x + threadIdx.x; wi < a.Wc; wi += gridDim.x * blockDim.x) {
+    uint32_t bits = 0u;
+    const int s0 = wi << 5;
+    const int n = min(32, a.L - s0);
+    for (int i = 0; i < n; ++i) {
+      const int s = s0 + i;
+      if (!a.lq[s] && !a.common[s] && H[s] != a.major[s]) bits |= 1u << i;
+    }
+    a.carry[(size_t)hp * a.Wc + wi] = bits;
+  }
+}
+
+// Any carrier bit in sites [k0, k1].
+__device__ __forceinline__ bool any_carrier(const uint32_t* __restrict__ c, int k0, int k1) {
+  const int w0 = k0 >> 5, w1 = k1 >> 5;
+  for (int w = w0; w <= w1; ++w) {
+    uint32_t v = c[w];
+    if (w == w0) v &= ~0u << (k0 & 31);
+    if (w == w1) v &= (k1 & 31) == 31 ? ~0u : ((1u << ((k1 & 31) + 1)) - 1u);
+    if (v) return true;
+  }
+  return false;
+}
+
 __global__ void k_pbwt_sweep(PbwtSelectArgs a) {
   const int hp = blockIdx.x * blockDim.x + threadIdx.x;
   if (hp >= a.n_haps) return;
@@ -110,6 +141,7 @@ __global__ void k_pbwt_sweep(PbwtSelectArgs a) {
   const int N = a.N, L = a.L, K = a.depth;
   const int t = a.hap_target[hp];
   const uint8_t* H = (a.hap_which[hp] ? a.h1 : a.h0) + (size_t)t * L;
+  const uint32_t* carry = a.carry + (size_t)hp * a.Wc;
   Pusher pu{a.push_key + (size_t)hp * K * a.cap, a.push_id + (size_t)hp * K * a.cap, a.push_cnt + (size_t)hp * K,
             a.cap, a.overflow};
   for (int o = 0; o < K; ++o) pu.cnt[o] = 0;
@@ -204,29 +236,28 @@ __global__ void k_pbwt_sweep(PbwtSelectArgs a) {
       const int sn = (int)(P.asoff[l + 1] - so);
       if (last_k < 0 || a.common[last_k]) {
         // init_rare: is this haplotype in rareTarHaps for the run?
-        in_rare = false;
-        if (sn > 0) {
-          for (int kk = k; kk < L; ++kk) {
-            if (a.lq[kk]) continue;
-            if (a.common[kk]) break;
-            if (H[kk] != a.major[kk]) {
-              in_rare = true;
-              break;
-            }
+        const int kend = max(P.run_end[k], k);  // the run start's own entry is always >= k
+        in_rare = sn > 0 && any_carrier(carry, k, kend);
+        // Nothing happens at the run's sites for a haplotype outside rareTarHaps.
+        // When no haplotype of the warp is in it, the warp continues after the run
+        // together, so that its lanes keep walking the sites in step.
+        if (__all_sync(__activemask(), !in_rare)) {
+          last_k = kend;
+          k = kend;
+          continue;
+        }
+        if (in_rare) {
+          const int32_t* sm = P.asidx + so;
+          int fsn = lower_count(sm, sn, f);
+          int gsn = lower_count(sm, sn, g);
+          if (gsn <= fsn) {
+            fsn = 0;
+            gsn = sn;
+            last_reset = k;
           }
-          if (in_rare) {
-            const int32_t* sm = P.asidx + so;
-            int fsn = lower_count(sm, sn, f);
-            int gsn = lower_count(sm, sn, g);
-            if (gsn <= fsn) {
-              fsn = 0;
-              gsn = sn;
-              last_reset = k;
-            }
-            sidx = lower_count(sm, sn, idx);
-            fs = fsn;
-            gs = gsn;
-          }
+          sidx = lower_count(sm, sn, idx);
+          fs = fsn;
+          gs = gsn;
         }
       }
       if (in_rare) {
@@ -317,6 +348,7 @@ __global__ void k_pbwt_union(PbwtSelectArgs a) {
 
 void launch_pbwt_select(const PbwtSelectArgs& a, cudaStream_t s) {
   k_pbwt_rng<<<1, 32, 0, s>>>(a);
+  k_rare_carriers<<<dim3((a.Wc + 127) / 128, a.n_haps), 128, 0, s>>>(a);
   k_pbwt_sweep<<<(a.n_haps + 63) / 64, 64, 0, s>>>(a);
   k_pbwt_union<<<(a.n_targets + 63) / 64, 64, 0, s>>>(a);
 }

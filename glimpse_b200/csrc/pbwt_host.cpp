@@ -225,7 +225,7 @@ int Context::pbwt_prepare_panel() {
   std::vector<uint32_t> merged_host;  // concatenated merged arrays
   std::vector<int64_t> svoff(1, 0);
   std::vector<uint32_t> svbits, svpref;
-  std::vector<int32_t> site_info(L, 0), site_run(L, 0), common2tot;
+  std::vector<int32_t> site_info(L, 0), site_run(L, 0), run_end(L, -1), common2tot;
   std::vector<uint32_t> A(N), B(N);
   std::iota(A.begin(), A.end(), 0u);
   std::vector<uint32_t> sA, sB;
@@ -275,7 +275,7 @@ int Context::pbwt_prepare_panel() {
   };
 
   int l_hq = 0, l_all = 0, last_k = -1, rare_ord = 0;
-  int run_l = -1;
+  int run_l = -1, run_k0 = -1;
   for (int k = 0; k < L; ++k) {
     if (host.common[k]) common2tot.push_back(k);
     if (host.lq[k]) {
@@ -315,6 +315,7 @@ int Context::pbwt_prepare_panel() {
       if (last_k < 0 || host.common[last_k]) {
         // init_rare (haplotype_set.cpp:655-662)
         run_l = l_hq;
+        run_k0 = k;
         const int64_t so = sparse.asmall_off[l_hq], sn = sparse.asmall_off[l_hq + 1] - so;
         sA.resize(sn);
         sB.resize(sn);
@@ -331,6 +332,7 @@ int Context::pbwt_prepare_panel() {
       svoff.push_back((int64_t)svbits.size());
       site_info[k] = SK_RARE | (rare_ord << 2);
       site_run[k] = run_l;
+      run_end[run_k0] = k;
       ++rare_ord;
     }
     last_k = k;
@@ -350,6 +352,7 @@ int Context::pbwt_prepare_panel() {
   if ((e = dev_upload(&D.asidx, sparse.asmall, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");
   if ((e = dev_upload(&D.site_info, site_info, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");
   if ((e = dev_upload(&D.site_run, site_run, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");
+  if ((e = dev_upload(&D.run_end, run_end, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");
   if ((e = dev_upload(&D.init_common, initc, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");
   if ((e = dev_upload(&D.cm_pos, cmp, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");
   if ((e = dev_upload(&D.common2tot, common2tot, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");
@@ -467,6 +470,12 @@ int Context::pbwt_select_states(int stage, int iteration, int Kp) {
   a.grp = T.d_grp.as<int32_t>();
   a.nstored = (int)pbwt_grp.size();
   a.stored_bits = T.stored_bits.as<uint32_t>();
+  a.Wc = (host.L + 31) / 32;
+  {
+    cudaError_t ec = T.carry.ensure((size_t)a.n_haps * a.Wc * 4);
+    if (ec != cudaSuccess) return cuda_fail(ec, "alloc carry");
+  }
+  a.carry = T.carry.as<uint32_t>();
   a.start_idx = T.start_idx.as<int32_t>();
   a.tar_hap = T.tar_hap.as<uint8_t>();
   a.push_key = T.push_key.as<uint32_t>();
@@ -482,7 +491,7 @@ int Context::pbwt_select_states(int stage, int iteration, int Kp) {
   a.iteration = iteration;
   cudaMemsetAsync(T.overflow.ptr, 0, 4, stream);
   launch_pbwt_select(a, stream);
-  prof.kernel_launches += 3;
+  prof.kernel_launches += 4;
   int32_t ovf = 0;
   cudaMemcpyAsync(&ovf, T.overflow.ptr, 4, cudaMemcpyDeviceToHost, stream);
   cudaError_t e = cudaStreamSynchronize(stream);

@@ -52,6 +52,7 @@ struct DevPbwt {
   int32_t* asidx = nullptr;
   int32_t* site_info = nullptr;  // [L]: kind | (index << 2); common: l_hq, rare: rare ordinal
   int32_t* site_run = nullptr;   // [L]: rare sites: run index l (A_small_idx row); common: l_all
+  int32_t* run_end = nullptr;    // [L]: at the first site of a run of rare sites, the run's last non-LQ site
   uint8_t* init_common = nullptr;  // [n_com_hq]
   uint32_t* cref = nullptr;      // [L]
   float* cm_pos = nullptr;       // [L]  max(0, (float)cm)
@@ -75,6 +76,8 @@ struct PbwtSelectArgs {
   const int32_t* grp;         // [nstored] group ends (pbwt_grp)
   int nstored;
   uint32_t* stored_bits;      // [ceil(n_com_hq/32)]
+  uint32_t* carry;            // [n_haps][Wc]: bit k = non-LQ rare site k where the haplotype has the non-major allele
+  int Wc;                     // ceil(L / 32)
   int32_t* start_idx;         // [n_haps] random pbwt_index
   uint8_t* tar_hap;           // [n_haps] persistent across iterations
   uint32_t* push_key;         // [n_haps][depth][cap]
