@@ -23,6 +23,8 @@
 // Sums follow a fixed order (lane-sequential over j, then a lane butterfly), so
 // results are deterministic. Every fused multiply-add is an explicit fmaf where
 // the reference's compiled arithmetic has one (build with --fmad=false).
+#include <type_traits>
+
 #include "internal.h"
 
 namespace gp {
@@ -115,7 +117,8 @@ __device__ __forceinline__ void chain_step(float (&x)[J], const uint32_t (&w)[J]
                                            float fact2, float ex, float ey, const float* rowl, float* srowl) {
 #pragma unroll
   for (int j0 = 0; j0 < J; j0 += 4) {
-    if (j0 < jn) {
+    if (j0 >= jn) break;  // jn is the same on every lane
+    {
 #pragma unroll
       for (int jj = 0; jj < 4; ++jj) {
         const int j = j0 + jj;
@@ -152,57 +155,62 @@ __device__ __forceinline__ void chain_step(float (&x)[J], const uint32_t (&w)[J]
 // Site bits: the 32-bit Hvar word of a state covers a 32-site block; it is kept
 // shifted so that the current site's bit is the sign bit (bit-reversed for the
 // forward direction), which turns the emission choice into a sign test.
-template <int J>
-__global__ void __launch_bounds__(32 * kWarpsPerCta) k_impute_warp(
-    int phase, int nchains, const int32_t* __restrict__ poly, const int32_t* __restrict__ npoly,
-    const int32_t* __restrict__ nstates, const uint32_t* __restrict__ hvar, const float4* __restrict__ em,
-    const float2* __restrict__ tr, const uint8_t* __restrict__ fl, const int64_t* __restrict__ store_off,
-    float* __restrict__ store_pool, WarpScratch sc, int L, int WB, int Kp, ModelConst mc, float* __restrict__ hp) {
-  static_assert(J % 4 == 0, "groups are processed in chunks of 4");
-  extern __shared__ __align__(16) char smem_raw[];
-  const int warp = threadIdx.x >> 5;
-  const int lane = threadIdx.x & 31;
-  const int chain = blockIdx.x * kWarpsPerCta + warp;
-  if (chain >= nchains) return;
-  const int t = chain >> 1;
-  const bool fwd = (chain & 1) == 0;
-  const int np = npoly[t];
-  const int K = nstates[t];
-  const int M = sc.split[t];
+// Arguments of one launch, shared by the forward and backward chains.
+struct ChainArgs {
+  int nchains;
+  const int32_t* __restrict__ poly;
+  const int32_t* __restrict__ npoly;
+  const int32_t* __restrict__ nstates;
+  const uint32_t* __restrict__ hvar;
+  const float4* __restrict__ em;
+  const float2* __restrict__ tr;
+  const uint8_t* __restrict__ fl;
+  const int64_t* __restrict__ store_off;
+  float* __restrict__ store_pool;
+  WarpScratch sc;
+  int L, WB, Kp;
+  ModelConst mc;
+  float* __restrict__ hp;
+};
+
+// One chain (a haplotype in one direction) over its sites [lo, hi), with the
+// direction FWD and the phase (POST = phase 2) fixed at compile time, so the
+// per-site loop carries no dispatch. The first site of a chain is peeled when it
+// starts the recursion (INIT).
+template <int J, bool FWD, bool POST>
+__device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, int t, int lane) {
+  const int np = A.npoly[t];
+  const int K = A.nstates[t];
+  const int M = A.sc.split[t];
   if (np == 0 || K == 0) return;
-  int lo, hi;
-  if (phase == 1) {
-    if (fwd) { lo = 0; hi = M; } else { lo = M; hi = np; }
-  } else {
-    if (fwd) { lo = M; hi = np; } else { lo = 0; hi = M; }
-  }
+  const int lo = (FWD == POST) ? M : 0;   // phase 1: forward [0, M), backward [M, np)
+  const int hi = (FWD == POST) ? np : M;  // phase 2: forward [M, np), backward [0, M)
   if (lo >= hi) return;
+  const int Kp = A.Kp;
   const int jn = (((K + 31) >> 5) + 3) & ~3;  // groups in use, a multiple of 4
   const int pad = 32 * jn - K;
   bool vg[4];                                 // validity of this lane in groups 0..3
 #pragma unroll
   for (int j = 0; j < 4; ++j) vg[j] = (32 * j + lane) >= pad;
   const int kb = lane - pad;                  // state index of group 0 for this lane
-  WarpSmem S = carve(smem_raw + (size_t)warp * warp_smem_bytes(Kp), Kp);
-  float* store = store_pool + store_off[t];
-  const uint32_t* hv = hvar + (size_t)t * WB * Kp;
-  const float4* E = em + (size_t)t * L;
-  const float2* T = tr + (size_t)t * L;
-  const uint8_t* F = fl + (size_t)t * L;
-  float* HP = hp + (size_t)t * 2 * L;
-  const int32_t* PL = poly + (size_t)t * L;
-  const bool post = (phase == 2);
+  WarpSmem S = carve(smem, Kp);
+  float* store = A.store_pool + A.store_off[t];
+  const uint32_t* hv = A.hvar + (size_t)t * A.WB * Kp;
+  const float4* E = A.em + (size_t)t * A.L;
+  const float2* T = A.tr + (size_t)t * A.L;
+  const uint8_t* F = A.fl + (size_t)t * A.L;
+  float* HP = A.hp + (size_t)t * 2 * A.L;
+  const int32_t* PL = A.poly + (size_t)t * A.L;
   const int n = hi - lo;
   const float Kf = (float)K;
-  auto site_of = [&](int s) { return fwd ? lo + s : hi - 1 - s; };
-  auto block_of = [&](int s) { return site_of(s) >> 5; };
+  auto site_of = [&](int s) { return FWD ? lo + s : hi - 1 - s; };
   // index of the value owned by (j, lane) in a K-long row; padding reads entry 0
   auto idx = [&](int j) { return max(32 * j + kb, 0); };
+  constexpr int dir = FWD ? 1 : -1;
 
-  // ---- prologue ----
-  const int b_first = block_of(0);
-  const int b_last = block_of(n - 1);
-  const int dir = fwd ? 1 : -1;
+  // ---- prologue: records and Hvar words of the first two blocks, first rows ----
+  const int b_first = site_of(0) >> 5;
+  const int b_last = site_of(n - 1) >> 5;
   {
     const int l = (b_first << 5) + lane;
     if (l < np) {
@@ -218,14 +226,16 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_impute_warp(
     }
   }
   cp_commit();
+  if (POST) {
 #pragma unroll
-  for (int d = 0; d < kRowDepth; ++d) {
-    if (post && d < n) copy_row_async<J>(S.ring + (size_t)(d % kRing) * Kp, store + (size_t)site_of(d) * Kp, Kp, lane);
-    cp_commit();
+    for (int d = 0; d < kRowDepth; ++d) {
+      if (d < n) copy_row_async<J>(S.ring + (size_t)(d % kRing) * Kp, store + (size_t)site_of(d) * Kp, Kp, lane);
+      cp_commit();
+    }
   }
 
   float x[J];      // alpha (forward) or Beta (backward)
-  uint32_t w[J];   // Hvar bits, current site in the sign bit
+  uint32_t w[J];   // Hvar words of the current block
 #pragma unroll
   for (int j = 0; j < J; ++j) {
     x[j] = 0.f;
@@ -233,18 +243,18 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_impute_warp(
   }
   float acc = 0.f;  // AlphaSum / betaSum of the previous step
   float2 t_prev = make_float2(0.f, 0.f);
-  if (fwd && lo > 0) {
+  if (FWD && lo > 0) {
 #pragma unroll
     for (int j = 0; j < J; ++j)
       if (j < jn) x[j] = (j >= 4 || vg[j & 3]) ? store[(size_t)(lo - 1) * Kp + idx(j)] : 0.f;
-    acc = sc.asum[t];
+    acc = A.sc.asum[t];
     t_prev = T[lo - 1];
   }
-  if (!fwd && hi < np) {
+  if (!FWD && hi < np) {
 #pragma unroll
     for (int j = 0; j < J; ++j)
-      if (j < jn) x[j] = (j >= 4 || vg[j & 3]) ? sc.brow[(size_t)t * Kp + idx(j)] : 0.f;
-    acc = sc.bsum[t];
+      if (j < jn) x[j] = (j >= 4 || vg[j & 3]) ? A.sc.brow[(size_t)t * Kp + idx(j)] : 0.f;
+    acc = A.sc.bsum[t];
   }
   float4 pe = make_float4(0.f, 0.f, 0.f, 0.f);
   float2 pt = make_float2(0.f, 0.f);
@@ -255,12 +265,14 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_impute_warp(
     if (ln < np) { pe = E[ln]; pt = T[ln]; pf = F[ln]; pp = PL[ln]; }
   }
   int cur_block = b_first;
+  if (!POST) cp_wait<0>();  // words of the first block (phase 2 waits per site below)
 
-  for (int s = 0; s < n; ++s) {
+  auto step = [&](int s, auto init_tag) {
+    constexpr bool INIT = decltype(init_tag)::value;
     const int l = site_of(s);
     const int b = l >> 5;
     const int i = l & 31;
-    const bool new_block = (s == 0) || (b != cur_block);
+    const bool new_block = INIT || (s == 0) || (b != cur_block);
     if (b != cur_block) {
       S.em[(b & 1) * 32 + lane] = pe;
       S.tr[(b & 1) * 32 + lane] = pt;
@@ -273,12 +285,18 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_impute_warp(
         if (ln < np) { pe = E[ln]; pt = T[ln]; pf = F[ln]; pp = PL[ln]; }
         copy_row_async<J>(S.words + (size_t)(bn & 1) * Kp, hv + (size_t)bn * Kp, Kp, lane);
       }
+      if (!POST) {
+        cp_commit();
+        cp_wait<1>();  // this block's words; the next block's may still be in flight
+      }
     }
-    if (post && s + kRowDepth < n)
-      copy_row_async<J>(S.ring + (size_t)((s + kRowDepth) % kRing) * Kp, store + (size_t)site_of(s + kRowDepth) * Kp,
-                     Kp, lane);
-    cp_commit();
-    cp_wait<kRowDepth>();
+    if (POST) {
+      if (s + kRowDepth < n)
+        copy_row_async<J>(S.ring + (size_t)((s + kRowDepth) % kRing) * Kp,
+                          store + (size_t)site_of(s + kRowDepth) * Kp, Kp, lane);
+      cp_commit();
+      cp_wait<kRowDepth>();
+    }
     __syncwarp();
     if (new_block) {
       const uint32_t* wbl = S.words + (size_t)(b & 1) * Kp + kb;
@@ -291,86 +309,113 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_impute_warp(
     const float4 e = S.em[(b & 1) * 32 + i];
     const float* rowl = S.ring + (size_t)(s % kRing) * Kp + kb;
     float* srowl = store + (size_t)l * Kp + kb;
-    const bool last = (l == np - 1);
     float q0[4] = {0.f, 0.f, 0.f, 0.f}, q1[4] = {0.f, 0.f, 0.f, 0.f}, q2[4] = {0.f, 0.f, 0.f, 0.f};
-    const bool init = fwd ? (l == 0) : last;
     float fact1, fact2;
-    if (fwd) {
-      fact1 = init ? 1.0f / Kf : t_prev.x;  // t_prev.x = t / K of the previous site
-      fact2 = init ? 0.f : t_prev.y / acc;
+    if (INIT) {
+      fact1 = 1.0f / Kf;
+      fact2 = 0.f;
+    } else if (FWD) {
+      fact1 = t_prev.x;  // t / K of the previous site
+      fact2 = t_prev.y / acc;
     } else {
       const float2 tt = S.tr[(b & 1) * 32 + i];
-      fact1 = init ? 1.0f / Kf : tt.x;
-      fact2 = init ? 0.f : tt.y / acc;
+      fact1 = tt.x;
+      fact2 = tt.y / acc;
     }
-    // one specialised state loop per (direction, phase, first/last site)
     const float ex = f ? 1.0f : e.x, ey = f ? 1.0f : e.y;
-#define GP_STEP(FWD, POST, INIT) \
-  chain_step<J, FWD, POST, INIT>(x, w, m, q0, q1, q2, vg, jn, fact1, fact2, ex, ey, rowl, srowl)
-    if (fwd) {
-      if (post) { if (init) GP_STEP(true, true, true); else GP_STEP(true, true, false); }
-      else { if (init) GP_STEP(true, false, true); else GP_STEP(true, false, false); }
-    } else {
-      if (post) { if (init) GP_STEP(false, true, true); else GP_STEP(false, true, false); }
-      else { if (init) GP_STEP(false, false, true); else GP_STEP(false, false, false); }
-    }
-#undef GP_STEP
+    chain_step<J, FWD, POST, INIT>(x, w, m, q0, q1, q2, vg, jn, fact1, fact2, ex, ey, rowl, srowl);
     const float v0 = warp_sum(__fadd_rn(__fadd_rn(q0[0], q0[1]), __fadd_rn(q0[2], q0[3])));
-    if (fwd) {
-      acc = (f && l == 0) ? 1.0f : v0;  // AlphaSum[0] = 1 at a flat first site (imputation_hmm.cpp:156)
-      t_prev = S.tr[(b & 1) * 32 + i];
-    } else {
-      acc = (f && last) ? 1.0f : v0;  // betaSum = 1 at a flat last site (imputation_hmm.cpp:285)
-    }
-    if (post) {
+    // AlphaSum = 1 at a flat first site, betaSum = 1 at a flat last site (imputation_hmm.cpp:156,285)
+    acc = (INIT && f) ? 1.0f : v0;
+    if (FWD) t_prev = S.tr[(b & 1) * 32 + i];
+    if (POST) {
       const float v1 = warp_sum(__fadd_rn(__fadd_rn(q1[0], q1[1]), __fadd_rn(q1[2], q1[3])));
       const float v2 = warp_sum(__fadd_rn(__fadd_rn(q2[0], q2[1]), __fadd_rn(q2[2], q2[3])));
       // prob_hid of the two alleles; k_impute_finish turns them into HP
       if (lane == 0) *reinterpret_cast<float2*>(HP + 2 * S.pl[(b & 1) * 32 + i]) = make_float2(v1, v2);
     }
     __syncwarp();
+  };
+
+  // The recursion starts at site 0 (forward) or np - 1 (backward) with 1/K.
+  const bool starts = FWD ? (lo == 0) : (hi == np);
+  int s0 = 0;
+  if (starts) {
+    step(0, std::integral_constant<bool, true>());
+    s0 = 1;
   }
+  for (int s = s0; s < n; ++s) step(s, std::integral_constant<bool, false>());
+
   cp_wait<0>();
-  if (!post) {
-    if (fwd) {
-      if (lane == 0) sc.asum[t] = acc;
+  if (!POST) {
+    if (FWD) {
+      if (lane == 0) A.sc.asum[t] = acc;
     } else {
 #pragma unroll
       for (int j = 0; j < J; ++j)
-        if (j < jn && (j >= 4 || vg[j & 3])) sc.brow[(size_t)t * Kp + idx(j)] = x[j];
-      if (lane == 0) sc.bsum[t] = acc;
+        if (j < jn && (j >= 4 || vg[j & 3])) A.sc.brow[(size_t)t * Kp + idx(j)] = x[j];
+      if (lane == 0) A.sc.bsum[t] = acc;
     }
   }
+}
+
+// Warp `warp` of the CTA runs chain blockIdx.x * kWarpsPerCta + warp: target
+// chain / 2, forward for even chains and backward for odd ones.
+template <int J, bool POST>
+__global__ void __launch_bounds__(32 * kWarpsPerCta) k_impute_warp(ChainArgs A) {
+  static_assert(J % 4 == 0, "groups are processed in chunks of 4");
+  extern __shared__ __align__(16) char smem_raw[];
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int chain = blockIdx.x * kWarpsPerCta + warp;
+  if (chain >= A.nchains) return;
+  char* smem = smem_raw + (size_t)warp * warp_smem_bytes(A.Kp);
+  if ((chain & 1) == 0) run_chain<J, true, POST>(A, smem, chain >> 1, lane);
+  else run_chain<J, false, POST>(A, smem, chain >> 1, lane);
 }
 
 }  // namespace
 
 size_t impute_warp_smem(int Kp) { return (size_t)kWarpsPerCta * warp_smem_bytes(Kp); }
 
-int launch_impute_warp(int phase, int J, const ModelConst& mc, ImputeWork& w, float* hp, cudaStream_t s) {
-  WarpScratch sc;
-  sc.asum = w.split_scr.as<float>();
-  sc.bsum = sc.asum + w.n;
-  sc.brow = sc.bsum + w.n;
-  sc.split = w.split.as<int32_t>();
-  const int nchains = 2 * w.n;
-  const dim3 g((nchains + kWarpsPerCta - 1) / kWarpsPerCta);
-  const size_t sm = impute_warp_smem(w.Kp);
-#define GP_WARP(JJ)                                                                                          \
-  case JJ: {                                                                                                 \
-    static bool attr = false;                                                                                \
-    if (!attr) {                                                                                             \
-      cudaFuncSetAttribute(k_impute_warp<JJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);      \
-      attr = true;                                                                                           \
-    }                                                                                                        \
-    k_impute_warp<JJ><<<g, 32 * kWarpsPerCta, sm, s>>>(phase, nchains, w.poly.as<int32_t>(),                 \
-                                                       w.npoly.as<int32_t>(), w.nstates.as<int32_t>(),       \
-                                                       w.hvar.as<uint32_t>(), w.em.as<float4>(),             \
-                                                       w.tr.as<float2>(), w.fl.as<uint8_t>(),                \
-                                                       w.alpha_off.as<int64_t>(), w.alpha.as<float>(), sc, w.L, \
-                                                       w.WB, w.Kp, mc, hp);                                  \
-    break;                                                                                                   \
+template <int J, bool POST>
+static void launch_chains(const ChainArgs& a, dim3 g, size_t sm, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_impute_warp<J, POST>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr = true;
   }
+  k_impute_warp<J, POST><<<g, 32 * kWarpsPerCta, sm, s>>>(a);
+}
+
+int launch_impute_warp(int phase, int J, const ModelConst& mc, ImputeWork& w, float* hp, cudaStream_t s) {
+  ChainArgs a;
+  a.sc.asum = w.split_scr.as<float>();
+  a.sc.bsum = a.sc.asum + w.n;
+  a.sc.brow = a.sc.bsum + w.n;
+  a.sc.split = w.split.as<int32_t>();
+  a.nchains = 2 * w.n;
+  a.poly = w.poly.as<int32_t>();
+  a.npoly = w.npoly.as<int32_t>();
+  a.nstates = w.nstates.as<int32_t>();
+  a.hvar = w.hvar.as<uint32_t>();
+  a.em = w.em.as<float4>();
+  a.tr = w.tr.as<float2>();
+  a.fl = w.fl.as<uint8_t>();
+  a.store_off = w.alpha_off.as<int64_t>();
+  a.store_pool = w.alpha.as<float>();
+  a.L = w.L;
+  a.WB = w.WB;
+  a.Kp = w.Kp;
+  a.mc = mc;
+  a.hp = hp;
+  const dim3 g((a.nchains + kWarpsPerCta - 1) / kWarpsPerCta);
+  const size_t sm = impute_warp_smem(w.Kp);
+#define GP_WARP(JJ)                                                           \
+  case JJ:                                                                    \
+    if (phase == 2) launch_chains<JJ, true>(a, g, sm, s);                     \
+    else launch_chains<JJ, false>(a, g, sm, s);                               \
+    break;
   switch (J) {
     GP_WARP(8) GP_WARP(16) GP_WARP(24) GP_WARP(32) GP_WARP(40) GP_WARP(48) GP_WARP(56) GP_WARP(64)
     default: return GP_E_ARG;

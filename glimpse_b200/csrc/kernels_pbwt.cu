@@ -10,6 +10,8 @@
 // that the union can rebuild the per-sample, per-level lists in the reference's
 // push order (sites in order, init_common before select_common, haplotypes in
 // order, down before up).
+#include <algorithm>
+
 #include "select.h"
 
 namespace gp {
@@ -32,26 +34,58 @@ __device__ __forceinline__ int lower_count(const int32_t* __restrict__ a, int n,
   return lo;
 }
 
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(smem))),
+               "l"(gmem));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_wait_all_but(int n) {
+  // wait until at most n of this thread's cp.async groups are pending (n < 8)
+  switch (n) {
+    case 0: asm volatile("cp.async.wait_group 0;\n" ::); break;
+    case 1: asm volatile("cp.async.wait_group 1;\n" ::); break;
+    case 2: asm volatile("cp.async.wait_group 2;\n" ::); break;
+    case 3: asm volatile("cp.async.wait_group 3;\n" ::); break;
+    case 4: asm volatile("cp.async.wait_group 4;\n" ::); break;
+    case 5: asm volatile("cp.async.wait_group 5;\n" ::); break;
+    case 6: asm volatile("cp.async.wait_group 6;\n" ::); break;
+    default: asm volatile("cp.async.wait_group 7;\n" ::); break;
+  }
+}
+
+// Warp-cooperative copy of one vrow row (R words, R a multiple of 4, 16-byte
+// aligned) into a ring slot, spread over the live lanes of the warp.
+__device__ __forceinline__ void stage_row(uint32_t* slot, const uint32_t* row, int R, int rank, int nlive) {
+  for (int c = rank; c < (R >> 2); c += nlive) cp_async16(slot + 4 * c, row + 4 * c);
+}
+
+// Per-level push lists of one target haplotype. The counts live in shared
+// memory (level-major, one column per lane) while the sweep runs and are
+// written back to push_cnt at its end.
 struct Pusher {
   uint32_t* key;
   uint32_t* id;
-  int32_t* cnt;
+  int32_t* cnt;  // shared: cnt[level * 32]
   int cap;
   int32_t* overflow;
-  __device__ void push(int level, uint32_t k, uint32_t h) {
-    const int c = cnt[level];
+  __device__ __forceinline__ void push(int level, uint32_t k, uint32_t h) {
+    const int c = cnt[level * 32];
     if (c >= cap) {
       *overflow = 1;
       return;
     }
     key[(size_t)level * cap + c] = k;
     id[(size_t)level * cap + c] = h;
-    cnt[level] = c + 1;
+    cnt[level * 32] = c + 1;
   }
 };
 
 // haplotype_set::selectK (haplotype_set.cpp:682-728); arr == nullptr means the
-// identity order.
+// identity order. The reference walks down (pbwt_idx, pbwt_idx + 1, ...) and up
+// (pbwt_idx - 1, ...) one level at a time and stops a side at its first position
+// outside [0, N) or on the other side of ref_rac than allele a; positions on the
+// allowed side of ref_rac form an interval, so each side pushes a run whose
+// length is known up front, and the loads of the run are independent.
 __device__ void select_k(int pbwt_idx, int f, int g, int ref_rac, const uint32_t* __restrict__ arr, int a, int K,
                          int N, uint32_t key, Pusher& P) {
   int nh_up = 0, nh_down = 0;
@@ -69,22 +103,22 @@ __device__ void select_k(int pbwt_idx, int f, int g, int ref_rac, const uint32_t
   } else if (d_down < k1) {
     nh_up += k1 - d_down;
   }
-  const int max_hh = max(nh_up, nh_down);
-  for (int o = 0, od = 0, ou = 0; o < max_hh; ++o) {
-    if (od < nh_down) {
-      const int idx = pbwt_idx + od;
-      if (idx < N && ((idx >= ref_rac) == (a != 0))) {
-        P.push(o, key, arr ? arr[idx] : (uint32_t)idx);
-        ++od;
-      }
-    }
-    if (ou < nh_up) {
-      const int idx = pbwt_idx - (ou + 1);
-      if (idx >= 0 && ((idx >= ref_rac) == (a != 0))) {
-        P.push(o, key, arr ? arr[idx] : (uint32_t)idx);
-        ++ou;
-      }
-    }
+  const bool alt = a != 0;
+  int cd = 0, cu = 0;
+  if (pbwt_idx >= 0 && pbwt_idx < N && ((pbwt_idx >= ref_rac) == alt)) {
+    const int lim = alt ? N : min(ref_rac, N);
+    cd = min(nh_down, lim - pbwt_idx);
+  }
+  const int p = pbwt_idx - 1;
+  if (p >= 0 && p < N && ((p >= ref_rac) == alt)) {
+    const int lo = alt ? max(ref_rac, 0) : 0;
+    cu = min(nh_up, p - lo + 1);
+  }
+  const int n = max(cd, cu);
+#pragma unroll 4
+  for (int o = 0; o < n; ++o) {
+    if (o < cd) P.push(o, key, arr ? arr[pbwt_idx + o] : (uint32_t)(pbwt_idx + o));
+    if (o < cu) P.push(o, key, arr ? arr[p - o] : (uint32_t)(p - o));
   }
 }
 
@@ -134,17 +168,33 @@ __device__ __forceinline__ bool any_carrier(const uint32_t* __restrict__ c, int 
   return false;
 }
 
-__global__ void k_pbwt_sweep(PbwtSelectArgs a) {
+// One warp per block; lane = one target haplotype. The lanes of a warp walk the
+// sites in step (every skip is warp-uniform), so the rank row of each HQ common
+// site is staged once per warp: a ring of D rows in shared memory is filled by
+// cp.async D common sites ahead of the one being processed. D = 0 reads the
+// rows from global memory (panels whose rows do not fit twice in shared memory).
+__global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D) {
+  extern __shared__ __align__(16) uint32_t ring[];  // [D][R]
   const int hp = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const unsigned live = __ballot_sync(0xffffffffu, hp < a.n_haps);
   if (hp >= a.n_haps) return;
+  const int rank = __popc(live & ((1u << lane) - 1u)), nlive = __popc(live);
   const DevPbwt& P = a.P;
+  const int R = P.R, Wv = P.Wv, ncom = P.n_com_hq;
+  if (D > 0) {
+    for (int j = 0; j < D; ++j) {
+      if (j < ncom) stage_row(ring + (size_t)j * R, P.vrow + (size_t)j * R, R, rank, nlive);
+      cp_commit();
+    }
+  }
   const int N = a.N, L = a.L, K = a.depth;
   const int t = a.hap_target[hp];
   const uint8_t* H = (a.hap_which[hp] ? a.h1 : a.h0) + (size_t)t * L;
   const uint32_t* carry = a.carry + (size_t)hp * a.Wc;
-  Pusher pu{a.push_key + (size_t)hp * K * a.cap, a.push_id + (size_t)hp * K * a.cap, a.push_cnt + (size_t)hp * K,
-            a.cap, a.overflow};
-  for (int o = 0; o < K; ++o) pu.cnt[o] = 0;
+  int32_t* scnt = reinterpret_cast<int32_t*>(ring + (size_t)D * R) + lane;  // [K][32]
+  Pusher pu{a.push_key + (size_t)hp * K * a.cap, a.push_id + (size_t)hp * K * a.cap, scnt, a.cap, a.overflow};
+  for (int o = 0; o < K; ++o) scnt[o * 32] = 0;
   int idx = a.start_idx[hp], f = 0, g = N;
   int sidx = 0, fs = 0, gs = 0;
   int last_reset = 0, last_rare = 0;
@@ -196,12 +246,26 @@ __global__ void k_pbwt_sweep(PbwtSelectArgs a) {
       }
       // select_common_pd_fg at HQ common site l
       const int ref = (int)P.cref[k];
-      const uint32_t* vb = P.vbits + (size_t)l * P.Wv;
-      const uint32_t* vp = P.vpref + (size_t)l * (P.Wv + 1);
       const int prev_hap = tar;
       const int al = H[k];
       tar = al;
-      const int vi = rank_v(vb, vp, idx), vf = rank_v(vb, vp, f), vg = rank_v(vb, vp, g);
+      int vi, vf, vg;
+      if (D > 0) {
+        uint32_t* slot = ring + (size_t)(l % D) * R;
+        cp_wait_all_but(D - 1);  // this lane's part of row l has landed
+        __syncwarp(live);        // and every other lane's
+        vi = rank_v(slot, slot + Wv, idx);
+        vf = rank_v(slot, slot + Wv, f);
+        vg = rank_v(slot, slot + Wv, g);
+        __syncwarp(live);        // the slot is free again
+        if (l + D < ncom) stage_row(slot, P.vrow + (size_t)(l + D) * R, R, rank, nlive);
+        cp_commit();
+      } else {
+        const uint32_t* vb = P.vrow + (size_t)l * R;
+        vi = rank_v(vb, vb + Wv, idx);
+        vf = rank_v(vb, vb + Wv, f);
+        vg = rank_v(vb, vb + Wv, g);
+      }
       int nidx = al ? ref + vi : idx - vi;
       int nf = al ? ref + vf : f - vf;
       int ng = al ? ref + vg : g - vg;
@@ -241,7 +305,7 @@ __global__ void k_pbwt_sweep(PbwtSelectArgs a) {
         // Nothing happens at the run's sites for a haplotype outside rareTarHaps.
         // When no haplotype of the warp is in it, the warp continues after the run
         // together, so that its lanes keep walking the sites in step.
-        if (__all_sync(__activemask(), !in_rare)) {
+        if (__all_sync(live, !in_rare)) {
           last_k = kend;
           k = kend;
           continue;
@@ -293,6 +357,8 @@ __global__ void k_pbwt_sweep(PbwtSelectArgs a) {
     }
     last_k = k;
   }
+  if (D > 0) cp_wait_all_but(0);
+  for (int o = 0; o < K; ++o) a.push_cnt[(size_t)hp * K + o] = scnt[o * 32];
   a.tar_hap[hp] = (uint8_t)tar;
 }
 
@@ -349,7 +415,16 @@ __global__ void k_pbwt_union(PbwtSelectArgs a) {
 void launch_pbwt_select(const PbwtSelectArgs& a, cudaStream_t s) {
   k_pbwt_rng<<<1, 32, 0, s>>>(a);
   k_rare_carriers<<<dim3((a.Wc + 127) / 128, a.n_haps), 128, 0, s>>>(a);
-  k_pbwt_sweep<<<(a.n_haps + 63) / 64, 64, 0, s>>>(a);
+  const size_t row_bytes = (size_t)a.P.R * 4;
+  int D = (int)std::min<size_t>(8, (96u << 10) / row_bytes);
+  if (D < 2) D = 0;
+  const size_t smem = (size_t)D * row_bytes + (size_t)a.depth * 32 * 4;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_pbwt_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 << 10);
+    attr = true;
+  }
+  k_pbwt_sweep<<<(a.n_haps + 31) / 32, 32, smem, s>>>(a, D);
   k_pbwt_union<<<(a.n_targets + 63) / 64, 64, 0, s>>>(a);
 }
 

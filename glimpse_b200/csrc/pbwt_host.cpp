@@ -214,11 +214,11 @@ int Context::pbwt_prepare_panel() {
   const int n_com_hq = host.n_com_hq;
   D.n_com_hq = n_com_hq;
   D.Wv = (N + 1 + 31) / 32;
-  const int Wv = D.Wv;
+  D.R = (2 * D.Wv + 1 + 3) / 4 * 4;  // 16-byte rows, staged by the sweep with cp.async
+  const int Wv = D.Wv, R = D.R;
   cudaError_t e;
   if ((e = dev_alloc(&D.a_after, (size_t)n_com_hq * N, owned)) != cudaSuccess) return cuda_fail(e, "alloc pbwt");
-  if ((e = dev_alloc(&D.vbits, (size_t)n_com_hq * Wv, owned)) != cudaSuccess) return cuda_fail(e, "alloc pbwt");
-  if ((e = dev_alloc(&D.vpref, (size_t)n_com_hq * (Wv + 1), owned)) != cudaSuccess) return cuda_fail(e, "alloc pbwt");
+  if ((e = dev_alloc(&D.vrow, (size_t)n_com_hq * R, owned)) != cudaSuccess) return cuda_fail(e, "alloc pbwt");
 
   std::vector<int32_t> before_id(n_com_hq, -1);
   std::vector<uint8_t> initc(n_com_hq, 0);
@@ -231,17 +231,14 @@ int Context::pbwt_prepare_panel() {
   std::vector<uint32_t> sA, sB;
   // staged upload of a_after / V rows
   const int chunk = std::max(1, (int)std::min<int64_t>(4096, (512ll << 20) / ((int64_t)N * 4 + 1)));
-  std::vector<uint32_t> stage_a((size_t)chunk * N), stage_vb((size_t)chunk * Wv), stage_vp((size_t)chunk * (Wv + 1));
+  std::vector<uint32_t> stage_a((size_t)chunk * N), stage_vr((size_t)chunk * R, 0u);
   int stage_first = 0, stage_n = 0;
   auto flush = [&]() -> cudaError_t {
     if (!stage_n) return cudaSuccess;
     cudaError_t x = cudaMemcpy(D.a_after + (size_t)stage_first * N, stage_a.data(), (size_t)stage_n * N * 4,
                                cudaMemcpyHostToDevice);
     if (x == cudaSuccess)
-      x = cudaMemcpy(D.vbits + (size_t)stage_first * Wv, stage_vb.data(), (size_t)stage_n * Wv * 4,
-                     cudaMemcpyHostToDevice);
-    if (x == cudaSuccess)
-      x = cudaMemcpy(D.vpref + (size_t)stage_first * (Wv + 1), stage_vp.data(), (size_t)stage_n * (Wv + 1) * 4,
+      x = cudaMemcpy(D.vrow + (size_t)stage_first * R, stage_vr.data(), (size_t)stage_n * R * 4,
                      cudaMemcpyHostToDevice);
     stage_first += stage_n;
     stage_n = 0;
@@ -301,8 +298,8 @@ int Context::pbwt_prepare_panel() {
         before_id[l_hq] = (l_hq == 0) ? -2 : -1;
       }
       if (stage_n == chunk && (e = flush()) != cudaSuccess) return cuda_fail(e, "pbwt upload");
-      uint32_t* vb = stage_vb.data() + (size_t)stage_n * Wv;
-      uint32_t* vp = stage_vp.data() + (size_t)stage_n * (Wv + 1);
+      uint32_t* vb = stage_vr.data() + (size_t)stage_n * R;
+      uint32_t* vp = vb + Wv;
       if (!decode(A, B, N, (int)host.cref[k], vb, vp, Wv))
         return (fail(GP_E_DATA, "sparse PBWT stream is malformed at site " + std::to_string(k)), GP_E_DATA);
       std::copy(A.begin(), A.end(), stage_a.begin() + (size_t)stage_n * N);

@@ -39,12 +39,11 @@ void build_sparse_pbwt(int N, int L, const uint8_t* lq, const uint8_t* common, c
 // where a run of rare sites ends, and the rank (V) arrays of every column.
 struct DevPbwt {
   bool ready = false;
-  int n_com_hq = 0, Wv = 0, n_rare_hq = 0;
+  int n_com_hq = 0, Wv = 0, R = 0, n_rare_hq = 0;  // R: words per vrow row, a multiple of 4
   uint32_t* a_after = nullptr;   // [n_com_hq][N]
   int32_t* before_id = nullptr;  // [n_com_hq]: -2 iota, -1 a_after[l-1], >= 0 merged[id]
   uint32_t* merged = nullptr;    // [n_merged][N]
-  uint32_t* vbits = nullptr;     // [n_com_hq][Wv]
-  uint32_t* vpref = nullptr;     // [n_com_hq][Wv + 1]
+  uint32_t* vrow = nullptr;      // [n_com_hq][R]: V bits (Wv words), then their prefix counts (Wv + 1 words)
   int64_t* svoff = nullptr;      // [n_rare_hq + 1] word offsets of small columns
   uint32_t* svbits = nullptr;    // small-column bits
   uint32_t* svpref = nullptr;    // small-column prefix counts (one more entry per column)
