@@ -110,6 +110,8 @@ int Context::create_panel(const gp_panel_desc& d) {
   const int N = d.n_ref_haps, L = d.n_sites;
   if (N <= 0 || L <= 0 || !d.cm || !d.cref || !d.calt || !d.lq || !d.flag_common || !d.major || !d.shap_off)
     return (fail(GP_E_ARG, "panel: missing array or empty panel"), GP_E_ARG);
+  if (L >= (1 << 24))
+    return (fail(GP_E_ARG, "panel: more than 16,777,215 sites in one chunk"), GP_E_ARG);  // 24-bit site fields
   host.N = N;
   host.L = L;
   host.cm.assign(d.cm, d.cm + L);
@@ -332,6 +334,8 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   if ((e = p.ytp.ensure((size_t)nb * L * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
   if ((e = p.ytn.ensure((size_t)nb * L * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
   if ((e = p.vflags.ensure((size_t)nb * L)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.recb.ensure((size_t)nb * L * 16)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.recf.ensure((size_t)nb * L * 16)) != cudaSuccess) return cuda_fail(e, "alloc vars");
   PhaseVars V;
   V.rel = p.rel.as<int32_t>();
   V.code = p.code.as<uint8_t>();
@@ -341,6 +345,8 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   V.yt_prev = p.ytp.as<float>();
   V.yt_next = p.ytn.as<float>();
   V.flags = p.vflags.as<uint8_t>();
+  V.recb = p.recb.as<int4>();
+  V.recf = p.recf.as<int4>();
   V.nvar = p.counts.as<int32_t>();
   V.nseg = V.nvar + nb;
   V.nmiss = V.nvar + 2 * nb;

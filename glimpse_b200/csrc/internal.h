@@ -74,10 +74,10 @@ struct ImputeWork {
 
 // Scratch of the phasing HMM.
 struct PhaseWork {
-  DevBuf rel, code, seg, miss, seg_start, counts, ytp, ytn, vflags;
+  DevBuf rel, code, seg, miss, seg_start, counts, ytp, ytn, vflags, recb, recf;
   DevBuf pprob, iprob, offs, pprob_sum, pprob_sumsum, iprob_sum, of1, dip, err;
   std::vector<DevBuf*> all() {
-    return {&rel, &code, &seg, &miss, &seg_start, &counts, &ytp, &ytn, &vflags, &pprob, &iprob, &offs,
+    return {&rel, &code, &seg, &miss, &seg_start, &counts, &ytp, &ytn, &vflags, &recb, &recf, &pprob, &iprob, &offs,
             &pprob_sum, &pprob_sumsum, &iprob_sum, &of1, &dip, &err};
   }
 };

@@ -139,7 +139,12 @@ __global__ void k_var_records(const int32_t* __restrict__ tsel, const int32_t* _
     const int seg = vseg[i];
     const int locus = i - sstart[seg];
     const int seglen = sstart[seg + 1] - sstart[seg];
-    V.flags[(size_t)b * L + i] = (uint8_t)((locus == 0 ? 1 : 0) | (locus == seglen - 1 ? 2 : 0));
+    const int fl = (locus == 0 ? 1 : 0) | (locus == seglen - 1 ? 2 : 0);
+    V.flags[(size_t)b * L + i] = (uint8_t)fl;
+    const int x = vrel[i] | ((int)V.code[(size_t)b * L + i] << 24) | (fl << 28);
+    const int miss = V.miss[(size_t)b * L + i];
+    V.recb[(size_t)b * L + i] = make_int4(x, seg, miss, __float_as_int(yn));
+    V.recf[(size_t)b * L + i] = make_int4(x, seg, miss, __float_as_int(yp));
   }
 }
 
@@ -324,43 +329,26 @@ __device__ __forceinline__ void site_step(int mode, int code, float (&prob)[J][8
   else site_update<J, 0>(prob, sumk, w, m, K, tid, e0, e1, yt, nt, sumH, sumT, red, buf);
 }
 
-// VAR records of 32 consecutive entries, double-buffered in shared memory.
+// Packed VAR records (PhaseVars::recb / recf) of 32 consecutive entries,
+// double-buffered in shared memory.
 struct VarStage {
-  int32_t l[2][32];
-  int32_t seg[2][32];
-  int32_t miss[2][32];
-  float ytp[2][32];
-  float ytn[2][32];
-  uint8_t code[2][32];
-  uint8_t flags[2][32];
+  int4 rec[2][32];
 };
 
 struct VarRec {
-  int32_t l, seg, miss;
-  float ytp, ytn;
-  uint8_t code, flags;
+  int l, code, fl, seg, miss;
+  float yt;
 };
 
-__device__ __forceinline__ VarRec load_rec(const PhaseVars& V, size_t base, int i) {
-  VarRec r;
-  r.l = V.rel[base + i];
-  r.seg = V.seg[base + i];
-  r.miss = V.miss[base + i];
-  r.ytp = V.yt_prev[base + i];
-  r.ytn = V.yt_next[base + i];
-  r.code = V.code[base + i];
-  r.flags = V.flags[base + i];
-  return r;
-}
-
-__device__ __forceinline__ void put_rec(VarStage& st, int buf, int lane, const VarRec& r) {
-  st.l[buf][lane] = r.l;
-  st.seg[buf][lane] = r.seg;
-  st.miss[buf][lane] = r.miss;
-  st.ytp[buf][lane] = r.ytp;
-  st.ytn[buf][lane] = r.ytn;
-  st.code[buf][lane] = r.code;
-  st.flags[buf][lane] = r.flags;
+__device__ __forceinline__ VarRec unpack_rec(int4 r) {
+  VarRec v;
+  v.l = r.x & 0xffffff;
+  v.code = (r.x >> 24) & 15;
+  v.fl = (r.x >> 28) & 3;
+  v.seg = r.y;
+  v.miss = r.z;
+  v.yt = __int_as_float(r.w);
+  return v;
 }
 
 // Hvar words of the poly block holding the current site, with the adjacent
@@ -447,24 +435,25 @@ __global__ void __launch_bounds__(PT, 2) k_phase(const int32_t* __restrict__ tse
   // ---------------- backward (phasing_hmm.cpp:193-245) ----------------
   if (nvb > 0) {
     const int lb = nvb - 1;
-    if (loader && (lb << 5) + tid < nv) put_rec(vs, lb & 1, tid, load_rec(V, vbase, (lb << 5) + tid));
+    if (loader && (lb << 5) + tid < nv) vs.rec[lb & 1][tid] = V.recb[vbase + (lb << 5) + tid];
   }
   __syncthreads();
   for (int vb = nvb - 1; vb >= 0; --vb) {
     const int cur = vb & 1;
-    VarRec pre;
+    int4 pre;
     const bool have_next = vb > 0;
-    if (loader && have_next) pre = load_rec(V, vbase, ((vb - 1) << 5) + tid);
+    if (loader && have_next) pre = V.recb[vbase + ((vb - 1) << 5) + tid];
     const int n_in = min(32, nv - (vb << 5));
     for (int ii = n_in - 1; ii >= 0; --ii) {
       const int i = (vb << 5) + ii;
-      const int l = vs.l[cur][ii];
+      const VarRec r = unpack_rec(vs.rec[cur][ii]);
+      const int l = r.l;
       wc.need(l >> 5, -1, hv, nblk_poly, Kp, K, tid);
-      const int code = vs.code[cur][ii];
+      const int code = r.code;
       const int typ = code & 7;
-      const int seg = vs.seg[cur][ii];
-      const int fl = vs.flags[cur][ii];
-      const float yt = vs.ytn[cur][ii];
+      const int seg = r.seg;
+      const int fl = r.fl;
+      const float yt = r.yt;
       const float nt = 1.0f - yt;
       const int mode = (i == nv - 1) ? 0 : ((fl & 2) ? 2 : 1);
       site_step<J>(mode, code, prob, sumk, wc.w, 1u << (l & 31), K, tid, sm.etab, yt, nt, sumH, sumT, sm.red, buf);
@@ -475,12 +464,12 @@ __global__ void __launch_bounds__(PT, 2) k_phase(const int32_t* __restrict__ tse
         if (tid == 0) PPSS[seg] = sumT;
       }
       if (typ == VT_FLAT) {
-        const int m = vs.miss[cur][ii];
+        const int m = r.miss;
         store_rows(IP + (size_t)m * K * 8);
         if (tid < 8) IPS[m * 8 + tid] = sumH[tid];
       }
     }
-    if (loader && have_next) put_rec(vs, cur ^ 1, tid, pre);
+    if (loader && have_next) vs.rec[cur ^ 1][tid] = pre;
     __syncthreads();
   }
   __syncthreads();
@@ -510,23 +499,24 @@ __global__ void __launch_bounds__(PT, 2) k_phase(const int32_t* __restrict__ tse
 
   // ---------------- forward (phasing_hmm.cpp:142-191) ----------------
   wc.cur = wc.nxt = -1;
-  if (nvb > 0 && loader && tid < nv) put_rec(vs, 0, tid, load_rec(V, vbase, tid));
+  if (nvb > 0 && loader && tid < nv) vs.rec[0][tid] = V.recf[vbase + tid];
   __syncthreads();
   for (int vb = 0; vb < nvb; ++vb) {
     const int cur = vb & 1;
-    VarRec pre;
+    int4 pre;
     const bool have_next = vb + 1 < nvb;
-    if (loader && have_next && ((vb + 1) << 5) + tid < nv) pre = load_rec(V, vbase, ((vb + 1) << 5) + tid);
+    if (loader && have_next && ((vb + 1) << 5) + tid < nv) pre = V.recf[vbase + ((vb + 1) << 5) + tid];
     const int n_in = min(32, nv - (vb << 5));
     for (int ii = 0; ii < n_in; ++ii) {
       const int i = (vb << 5) + ii;
-      const int l = vs.l[cur][ii];
+      const VarRec r = unpack_rec(vs.rec[cur][ii]);
+      const int l = r.l;
       wc.need(l >> 5, 1, hv, nblk_poly, Kp, K, tid);
-      const int code = vs.code[cur][ii];
+      const int code = r.code;
       const int typ = code & 7;
-      const int seg = vs.seg[cur][ii];
-      const int fl = vs.flags[cur][ii];
-      const float yt = vs.ytp[cur][ii];
+      const int seg = r.seg;
+      const int fl = r.fl;
+      const float yt = r.yt;
       const float nt = 1.0f - yt;
       const int mode = (i == 0) ? 0 : ((fl & 1) ? 2 : 1);
       site_step<J>(mode, code, prob, sumk, wc.w, 1u << (l & 31), K, tid, sm.etab, yt, nt, sumH, sumT, sm.red, buf);
@@ -534,7 +524,7 @@ __global__ void __launch_bounds__(PT, 2) k_phase(const int32_t* __restrict__ tse
       if (seg_end) do_sumk();
       if (seg_end && i != nv - 1) {
         // TRANS_HAP (phasing_hmm.h:376-397)
-        const float yt2 = vs.ytn[cur][ii];
+        const float yt2 = V.yt_next[vbase + i];
         const float nt2 = 1.0f - yt2;
         const float fact2 = nt2 / sumT;
         const float* nxt = PP + (size_t)(seg + 1) * K * 8;
@@ -596,7 +586,7 @@ __global__ void __launch_bounds__(PT, 2) k_phase(const int32_t* __restrict__ tse
       }
       if (typ == VT_FLAT) {
         // IMPUTE_FLAT_HET (phasing_hmm.h:414-447)
-        const int m = vs.miss[cur][ii];
+        const int m = r.miss;
         const float* src = IP + (size_t)m * K * 8;
         float sR[8], sL[8];
 #pragma unroll
@@ -632,7 +622,7 @@ __global__ void __launch_bounds__(PT, 2) k_phase(const int32_t* __restrict__ tse
         }
       }
     }
-    if (loader && have_next && ((vb + 1) << 5) + tid < nv) put_rec(vs, cur ^ 1, tid, pre);
+    if (loader && have_next && ((vb + 1) << 5) + tid < nv) vs.rec[cur ^ 1][tid] = pre;
     __syncthreads();
   }
   if (tid == 0) S.err[b] = sm.err;

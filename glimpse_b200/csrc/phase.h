@@ -20,6 +20,11 @@ struct PhaseVars {
   float* yt_prev;      // transition from the previous VAR site (0 for the first)
   float* yt_next;      // transition to the next VAR site (0 for the last)
   uint8_t* flags;      // bit0: first entry of its segment, bit1: last entry of its segment
+  // The fields the sweeps read per entry, packed into 16 bytes per direction:
+  // x = rel | code << 24 | flags << 28, y = seg, z = miss, w = bits of the
+  // transition to the next entry (recb, backward) or from the previous one (recf).
+  int4* recb;
+  int4* recf;
   int32_t* nvar;
   int32_t* nseg;
   int32_t* nmiss;
