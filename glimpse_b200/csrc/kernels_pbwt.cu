@@ -38,6 +38,10 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(smem))),
                "l"(gmem));
 }
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(smem))),
+               "l"(gmem));
+}
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_wait_all_but(int n) {
   // wait until at most n of this thread's cp.async groups are pending (n < 8)
@@ -169,30 +173,72 @@ __device__ __forceinline__ bool any_carrier(const uint32_t* __restrict__ c, int 
 }
 
 // One warp per block; lane = one target haplotype. The lanes of a warp walk the
-// sites in step (every skip is warp-uniform), so the rank row of each HQ common
-// site is staged once per warp: a ring of D rows in shared memory is filled by
-// cp.async D common sites ahead of the one being processed. D = 0 reads the
-// rows from global memory (panels whose rows do not fit twice in shared memory).
-__global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D) {
-  extern __shared__ __align__(16) uint32_t ring[];  // [D][R]
+// event list (non-LQ common sites and runs of rare sites) in step: every branch
+// that skips work is warp-uniform. Shared memory per warp holds
+//   ring    D slots, one per HQ common site l, filled by cp.async D common sites
+//           ahead: the rank row of l (R words) and, when it has at most SEG
+//           entries, the run's small-PBWT index list asidx[asoff[l] ..) that the
+//           init_common searches at l read;
+//   evbuf   two chunks of 32 event records (the next chunk is loaded one chunk ahead);
+//   scnt    the per-level push counts, one column per lane.
+// D = 0 reads rows and index lists from global memory (panels whose rows do not
+// fit in shared memory).
+__global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D, int SEG) {
+  extern __shared__ __align__(16) uint32_t smem[];
   const int hp = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const unsigned live = __ballot_sync(0xffffffffu, hp < a.n_haps);
   if (hp >= a.n_haps) return;
   const int rank = __popc(live & ((1u << lane) - 1u)), nlive = __popc(live);
   const DevPbwt& P = a.P;
-  const int R = P.R, Wv = P.Wv, ncom = P.n_com_hq;
+  const int R = P.R, Wv = P.Wv, ncom = P.n_com_hq, nev = P.n_events;
+  const int SS = R + SEG;  // slot stride in words, a multiple of 4
+  const int N = a.N, K = a.depth;
+  uint32_t* ring = smem;
+  int4* evbuf = reinterpret_cast<int4*>(smem + (size_t)D * SS);  // [2][32][2]
+  int32_t* scnt = reinterpret_cast<int32_t*>(evbuf + 2 * 32 * 2) + lane;  // [K][32]
+
+  // slot of HQ common site l: rank row and (short) index list
+  auto stage = [&](int l, int so, int sn) {
+    uint32_t* slot = ring + (size_t)(l % D) * SS;
+    stage_row(slot, P.vrow + (size_t)l * R, R, rank, nlive);
+    if (sn <= SEG)
+      for (int i = rank; i < sn; i += nlive) cp_async4(slot + R + i, P.asidx + so + i);
+  };
+  int pf_so = 0, pf_sn = 0;  // index list of the next site to stage (l + D)
   if (D > 0) {
     for (int j = 0; j < D; ++j) {
-      if (j < ncom) stage_row(ring + (size_t)j * R, P.vrow + (size_t)j * R, R, rank, nlive);
+      if (j < ncom) {
+        const int so = P.asoff32[j];
+        stage(j, so, P.asoff32[j + 1] - so);
+      }
       cp_commit();
     }
+    if (D < ncom) {
+      pf_so = P.asoff32[D];
+      pf_sn = P.asoff32[D + 1] - pf_so;
+    }
   }
-  const int N = a.N, L = a.L, K = a.depth;
+  // Event chunk c (32 records) goes to evbuf[c & 1], spread over the live lanes
+  // (the last warp of the grid may have fewer than 32); chunk c + 1 is loaded
+  // when chunk c starts.
+  auto load_chunk = [&](int c) {
+    for (int i = rank; i < 32; i += nlive) {
+      const int en = (c << 5) + i;
+      if (en < nev) {
+        evbuf[((c & 1) * 32 + i) * 2] = P.events[2 * en];
+        evbuf[((c & 1) * 32 + i) * 2 + 1] = P.events[2 * en + 1];
+      }
+    }
+  };
+  load_chunk(0);
+  load_chunk(1);
+  __syncwarp(live);
+
+  const int L = a.L;
   const int t = a.hap_target[hp];
   const uint8_t* H = (a.hap_which[hp] ? a.h1 : a.h0) + (size_t)t * L;
   const uint32_t* carry = a.carry + (size_t)hp * a.Wc;
-  int32_t* scnt = reinterpret_cast<int32_t*>(ring + (size_t)D * R) + lane;  // [K][32]
   Pusher pu{a.push_key + (size_t)hp * K * a.cap, a.push_id + (size_t)hp * K * a.cap, scnt, a.cap, a.overflow};
   for (int o = 0; o < K; ++o) scnt[o * 32] = 0;
   int idx = a.start_idx[hp], f = 0, g = N;
@@ -201,20 +247,29 @@ __global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D) {
   int tar = a.tar_hap[hp];
   bool in_rare = false;
   int prev_ref_com = 0;
-  int last_k = -1;
   const float half_mod = a.modulo / 2.0f;
   const float fifth_mod = a.modulo / 5.0f;
-  for (int k = 0; k < L; ++k) {
-    const int info = P.site_info[k];
-    const int kind = info & 3;
-    if (kind == SK_LQ) continue;
-    if (kind == SK_COMMON) {
-      const int l = info >> 2;
+
+  for (int e = 0; e < nev; ++e) {
+    const int c = e >> 5;
+    if ((e & 31) == 0 && e > 0) {
+      __syncwarp(live);  // chunk c - 1 is no longer read
+      load_chunk(c + 1);
+    }
+    const int4 r0 = evbuf[((c & 1) * 32 + (e & 31)) * 2];
+    const int4 r1 = evbuf[((c & 1) * 32 + (e & 31)) * 2 + 1];
+    const int sn = r1.x;
+    if (!(r0.x & (1 << 30))) {
+      // ---------------- HQ common site ----------------
+      const int k = r0.x, l = r0.y, ref = r0.z, so = r0.w;
       const uint32_t* a_pre = l > 0 ? P.a_after + (size_t)(l - 1) * N : nullptr;
-      if (P.init_common[l]) {
-        const int64_t so = P.asoff[l];
-        const int sn = (int)(P.asoff[l + 1] - so);
-        const int32_t* sm = P.asidx + so;
+      uint32_t* slot = nullptr;
+      if (D > 0) {
+        slot = ring + (size_t)(l % D) * SS;
+        cp_wait_all_but(D - 1);  // this lane's part of slot l has landed
+        __syncwarp(live);        // and every other lane's
+      }
+      if (r1.z) {  // init_common
         int nidx, nf, ng;
         if (in_rare) {
           nidx = N - sn + sidx;
@@ -227,12 +282,13 @@ __global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D) {
             last_reset = k - 1;
           }
         } else {
+          const int32_t* sm = (D > 0 && sn <= SEG) ? reinterpret_cast<const int32_t*>(slot + R) : P.asidx + so;
           const int c0 = lower_count(sm, sn, f), c1 = lower_count(sm, sn, g), c2 = lower_count(sm, sn, idx);
           nidx = idx - c2;
           nf = f - c0;
           ng = g - c1;
           if (ng <= nf) {
-            const int prev_site = P.common2tot[l > 0 ? l - 1 : 0];  // indexed by the HQ count, as the reference does
+            const int prev_site = r1.w;  // common2tot indexed by the HQ count, as the reference does
             if (__fsub_rn(P.cm_pos[prev_site], P.cm_pos[last_reset]) > fifth_mod)
               select_k(idx, f, g, prev_ref_com, a_pre, tar, K, N, (uint32_t)(k << 1), pu);
             nf = 0;
@@ -245,20 +301,22 @@ __global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D) {
         g = ng;
       }
       // select_common_pd_fg at HQ common site l
-      const int ref = (int)P.cref[k];
       const int prev_hap = tar;
       const int al = H[k];
       tar = al;
       int vi, vf, vg;
       if (D > 0) {
-        uint32_t* slot = ring + (size_t)(l % D) * R;
-        cp_wait_all_but(D - 1);  // this lane's part of row l has landed
-        __syncwarp(live);        // and every other lane's
         vi = rank_v(slot, slot + Wv, idx);
         vf = rank_v(slot, slot + Wv, f);
         vg = rank_v(slot, slot + Wv, g);
-        __syncwarp(live);        // the slot is free again
-        if (l + D < ncom) stage_row(slot, P.vrow + (size_t)(l + D) * R, R, rank, nlive);
+        __syncwarp(live);  // the slot is free again
+        if (l + D < ncom) {
+          stage(l + D, pf_so, pf_sn);
+          if (l + D + 1 < ncom) {
+            pf_so = P.asoff32[l + D + 1];
+            pf_sn = P.asoff32[l + D + 2] - pf_so;
+          }
+        }
         cp_commit();
       } else {
         const uint32_t* vb = P.vrow + (size_t)l * R;
@@ -274,7 +332,7 @@ __global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D) {
       if (ng <= nf) {
         const int km1 = k > 0 ? k - 1 : 0;
         if (stored || __fsub_rn(P.cm_pos[km1], P.cm_pos[last_reset]) > half_mod) {
-          const int bid = P.before_id[l];
+          const int bid = r1.y;
           const uint32_t* b_arr = bid >= 0 ? P.merged + (size_t)bid * N : (bid == -1 ? a_pre : nullptr);
           select_k(idx, f, g, prev_ref_com, b_arr, prev_hap, K, N, (uint32_t)((k << 1) | 1), pu);
         }
@@ -294,37 +352,31 @@ __global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D) {
       }
       prev_ref_com = ref;
     } else {
-      const int r = info >> 2;
-      const int l = P.site_run[k];
-      const int64_t so = P.asoff[l];
-      const int sn = (int)(P.asoff[l + 1] - so);
-      if (last_k < 0 || a.common[last_k]) {
-        // init_rare: is this haplotype in rareTarHaps for the run?
-        const int kend = max(P.run_end[k], k);  // the run start's own entry is always >= k
-        in_rare = sn > 0 && any_carrier(carry, k, kend);
-        // Nothing happens at the run's sites for a haplotype outside rareTarHaps.
-        // When no haplotype of the warp is in it, the warp continues after the run
-        // together, so that its lanes keep walking the sites in step.
-        if (__all_sync(live, !in_rare)) {
-          last_k = kend;
-          k = kend;
-          continue;
-        }
-        if (in_rare) {
-          const int32_t* sm = P.asidx + so;
-          int fsn = lower_count(sm, sn, f);
-          int gsn = lower_count(sm, sn, g);
-          if (gsn <= fsn) {
-            fsn = 0;
-            gsn = sn;
-            last_reset = k;
-          }
-          sidx = lower_count(sm, sn, idx);
-          fs = fsn;
-          gs = gsn;
-        }
-      }
+      // ---------------- run of rare sites [k0, kend] ----------------
+      const int k0 = r0.x & ~(1 << 30), kend = r0.z, so = r0.w;
+      // init_rare: is this haplotype in rareTarHaps for the run?
+      in_rare = sn > 0 && any_carrier(carry, k0, kend);
+      // Nothing happens at the run's sites for a haplotype outside rareTarHaps;
+      // when no haplotype of the warp is in it, the warp goes on to the next event.
+      if (__all_sync(live, !in_rare)) continue;
       if (in_rare) {
+        const int32_t* sm = P.asidx + so;
+        int fsn = lower_count(sm, sn, f);
+        int gsn = lower_count(sm, sn, g);
+        if (gsn <= fsn) {
+          fsn = 0;
+          gsn = sn;
+          last_reset = k0;
+        }
+        sidx = lower_count(sm, sn, idx);
+        fs = fsn;
+        gs = gsn;
+      }
+      for (int k = k0; k <= kend; ++k) {
+        const int info = P.site_info[k];
+        if ((info & 3) == SK_LQ) continue;
+        if (!in_rare) continue;
+        const int r = info >> 2;
         const int ref = a.major[k] ? (int)P.cref[k] : sn - (int)a.calt[k];
         const uint32_t* vb = P.svbits + P.svoff[r];
         const uint32_t* vp = P.svpref + (P.svoff[r] + r);
@@ -355,7 +407,6 @@ __global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D) {
         gs = ngs;
       }
     }
-    last_k = k;
   }
   if (D > 0) cp_wait_all_but(0);
   for (int o = 0; o < K; ++o) a.push_cnt[(size_t)hp * K + o] = scnt[o * 32];
@@ -415,16 +466,18 @@ __global__ void k_pbwt_union(PbwtSelectArgs a) {
 void launch_pbwt_select(const PbwtSelectArgs& a, cudaStream_t s) {
   k_pbwt_rng<<<1, 32, 0, s>>>(a);
   k_rare_carriers<<<dim3((a.Wc + 127) / 128, a.n_haps), 128, 0, s>>>(a);
-  const size_t row_bytes = (size_t)a.P.R * 4;
-  int D = (int)std::min<size_t>(8, (96u << 10) / row_bytes);
+  // Ring of D slots (rank row + an index list of at most SEG entries), D <= 8, within 96 KB.
+  const int SEG = 256;
+  const size_t slot_bytes = ((size_t)a.P.R + SEG) * 4;
+  int D = (int)std::min<size_t>(8, (96u << 10) / slot_bytes);
   if (D < 2) D = 0;
-  const size_t smem = (size_t)D * row_bytes + (size_t)a.depth * 32 * 4;
+  const size_t smem = (size_t)D * slot_bytes + 2 * 32 * 2 * 16 + (size_t)a.depth * 32 * 4;
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_pbwt_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 << 10);
     attr = true;
   }
-  k_pbwt_sweep<<<(a.n_haps + 31) / 32, 32, smem, s>>>(a, D);
+  k_pbwt_sweep<<<(a.n_haps + 31) / 32, 32, smem, s>>>(a, D, SEG);
   k_pbwt_union<<<(a.n_targets + 63) / 64, 64, 0, s>>>(a);
 }
 

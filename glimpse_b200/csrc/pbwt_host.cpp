@@ -350,6 +350,33 @@ int Context::pbwt_prepare_panel() {
   if ((e = dev_upload(&D.site_info, site_info, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");
   if ((e = dev_upload(&D.site_run, site_run, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");
   if ((e = dev_upload(&D.run_end, run_end, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");
+  {
+    if (sparse.asmall_off.back() >= ((int64_t)1 << 31))
+      return (fail(GP_E_DATA, "sparse PBWT: small-column index list exceeds 2^31 entries"), GP_E_DATA);
+    std::vector<int32_t> ev, aoff32(sparse.asmall_off.begin(), sparse.asmall_off.end());
+    for (int k = 0; k < L; ++k) {
+      if (host.lq[k]) continue;
+      const int kind = site_info[k] & 3;
+      if (kind == SK_COMMON) {
+        const int l = site_info[k] >> 2;
+        const int64_t so = sparse.asmall_off[l], sn = sparse.asmall_off[l + 1] - so;
+        const int32_t a0[8] = {k, l, (int32_t)host.cref[k], (int32_t)so,
+                               (int32_t)sn, before_id[l], (int32_t)initc[l], common2tot[l > 0 ? l - 1 : 0]};
+        ev.insert(ev.end(), a0, a0 + 8);
+      } else if (run_end[k] >= 0) {
+        const int l = site_run[k];
+        const int64_t so = sparse.asmall_off[l], sn = sparse.asmall_off[l + 1] - so;
+        const int32_t a0[8] = {k | (1 << 30), l, run_end[k], (int32_t)so, (int32_t)sn, 0, 0, 0};
+        ev.insert(ev.end(), a0, a0 + 8);
+        k = run_end[k];
+      }
+    }
+    D.n_events = (int)(ev.size() / 8);
+    int32_t* evd = nullptr;
+    if ((e = dev_upload(&evd, ev, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");
+    D.events = reinterpret_cast<int4*>(evd);
+    if ((e = dev_upload(&D.asoff32, aoff32, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");
+  }
   if ((e = dev_upload(&D.init_common, initc, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");
   if ((e = dev_upload(&D.cm_pos, cmp, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");
   if ((e = dev_upload(&D.common2tot, common2tot, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");

@@ -52,6 +52,13 @@ struct DevPbwt {
   int32_t* site_info = nullptr;  // [L]: kind | (index << 2); common: l_hq, rare: rare ordinal
   int32_t* site_run = nullptr;   // [L]: rare sites: run index l (A_small_idx row); common: l_all
   int32_t* run_end = nullptr;    // [L]: at the first site of a run of rare sites, the run's last non-LQ site
+  // The sweep's event list: every non-LQ common site and every run of rare sites,
+  // in site order, as two int4 per event:
+  //   common: {k, l, cref[k], asoff[l]}, {sn(l), before_id[l], init_common[l], common2tot[max(l - 1, 0)]}
+  //   run:    {k | 1 << 30, l, last site of the run, asoff[l]}, {sn(l), 0, 0, 0}
+  int4* events = nullptr;
+  int n_events = 0;
+  int32_t* asoff32 = nullptr;    // [n_com_hq + 2] asoff as int32
   uint8_t* init_common = nullptr;  // [n_com_hq]
   uint32_t* cref = nullptr;      // [L]
   float* cm_pos = nullptr;       // [L]  max(0, (float)cm)
