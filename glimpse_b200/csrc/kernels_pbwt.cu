@@ -38,10 +38,6 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(smem))),
                "l"(gmem));
 }
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(smem))),
-               "l"(gmem));
-}
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_wait_all_but(int n) {
   // wait until at most n of this thread's cp.async groups are pending (n < 8)
@@ -176,14 +172,13 @@ __device__ __forceinline__ bool any_carrier(const uint32_t* __restrict__ c, int 
 // event list (non-LQ common sites and runs of rare sites) in step: every branch
 // that skips work is warp-uniform. Shared memory per warp holds
 //   ring    D slots, one per HQ common site l, filled by cp.async D common sites
-//           ahead: the rank row of l (R words) and, when it has at most SEG
-//           entries, the run's small-PBWT index list asidx[asoff[l] ..) that the
-//           init_common searches at l read;
+//           ahead with the rank row of l (R words: the V ranks of
+//           select_common_pd_fg and the small-PBWT position ranks of init_common);
 //   evbuf   two chunks of 32 event records (the next chunk is loaded one chunk ahead);
 //   scnt    the per-level push counts, one column per lane.
-// D = 0 reads rows and index lists from global memory (panels whose rows do not
-// fit in shared memory).
-__global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D, int SEG) {
+// D = 0 reads the rows from global memory (panels whose rows do not fit in
+// shared memory).
+__global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D) {
   extern __shared__ __align__(16) uint32_t smem[];
   const int hp = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
@@ -192,33 +187,18 @@ __global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D, int 
   const int rank = __popc(live & ((1u << lane) - 1u)), nlive = __popc(live);
   const DevPbwt& P = a.P;
   const int R = P.R, Wv = P.Wv, ncom = P.n_com_hq, nev = P.n_events;
-  const int SS = R + SEG;  // slot stride in words, a multiple of 4
   const int N = a.N, K = a.depth;
   uint32_t* ring = smem;
-  int4* evbuf = reinterpret_cast<int4*>(smem + (size_t)D * SS);  // [2][32][2]
+  int4* evbuf = reinterpret_cast<int4*>(smem + (size_t)D * R);  // [2][32][2]
   int32_t* scnt = reinterpret_cast<int32_t*>(evbuf + 2 * 32 * 2) + lane;  // [K][32]
 
-  // slot of HQ common site l: rank row and (short) index list
-  auto stage = [&](int l, int so, int sn) {
-    uint32_t* slot = ring + (size_t)(l % D) * SS;
-    stage_row(slot, P.vrow + (size_t)l * R, R, rank, nlive);
-    if (sn <= SEG)
-      for (int i = rank; i < sn; i += nlive) cp_async4(slot + R + i, P.asidx + so + i);
-  };
-  int pf_so = 0, pf_sn = 0;  // index list of the next site to stage (l + D)
   if (D > 0) {
     for (int j = 0; j < D; ++j) {
-      if (j < ncom) {
-        const int so = P.asoff32[j];
-        stage(j, so, P.asoff32[j + 1] - so);
-      }
+      if (j < ncom) stage_row(ring + (size_t)j * R, P.vrow + (size_t)j * R, R, rank, nlive);
       cp_commit();
     }
-    if (D < ncom) {
-      pf_so = P.asoff32[D];
-      pf_sn = P.asoff32[D + 1] - pf_so;
-    }
   }
+  int ri = 0;  // ring slot of the next HQ common site
   // Event chunk c (32 records) goes to evbuf[c & 1], spread over the live lanes
   // (the last warp of the grid may have fewer than 32); chunk c + 1 is loaded
   // when chunk c starts.
@@ -261,11 +241,14 @@ __global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D, int 
     const int sn = r1.x;
     if (!(r0.x & (1 << 30))) {
       // ---------------- HQ common site ----------------
-      const int k = r0.x, l = r0.y, ref = r0.z, so = r0.w;
+      const int k = r0.x, l = r0.y, ref = r0.z;
       const uint32_t* a_pre = l > 0 ? P.a_after + (size_t)(l - 1) * N : nullptr;
+      // rank row of l: the ring slot, or global memory without a ring
+      const uint32_t* row = P.vrow + (size_t)l * R;
       uint32_t* slot = nullptr;
       if (D > 0) {
-        slot = ring + (size_t)(l % D) * SS;
+        slot = ring + (size_t)ri * R;
+        row = slot;
         cp_wait_all_but(D - 1);  // this lane's part of slot l has landed
         __syncwarp(live);        // and every other lane's
       }
@@ -282,8 +265,9 @@ __global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D, int 
             last_reset = k - 1;
           }
         } else {
-          const int32_t* sm = (D > 0 && sn <= SEG) ? reinterpret_cast<const int32_t*>(slot + R) : P.asidx + so;
-          const int c0 = lower_count(sm, sn, f), c1 = lower_count(sm, sn, g), c2 = lower_count(sm, sn, idx);
+          // numbers of small-PBWT positions below f, g and idx: ranks in the row's second bit vector
+          const uint32_t* sb = row + 2 * Wv + 1;
+          const int c0 = rank_v(sb, sb + Wv, f), c1 = rank_v(sb, sb + Wv, g), c2 = rank_v(sb, sb + Wv, idx);
           nidx = idx - c2;
           nf = f - c0;
           ng = g - c1;
@@ -304,25 +288,12 @@ __global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D, int 
       const int prev_hap = tar;
       const int al = H[k];
       tar = al;
-      int vi, vf, vg;
+      const int vi = rank_v(row, row + Wv, idx), vf = rank_v(row, row + Wv, f), vg = rank_v(row, row + Wv, g);
       if (D > 0) {
-        vi = rank_v(slot, slot + Wv, idx);
-        vf = rank_v(slot, slot + Wv, f);
-        vg = rank_v(slot, slot + Wv, g);
         __syncwarp(live);  // the slot is free again
-        if (l + D < ncom) {
-          stage(l + D, pf_so, pf_sn);
-          if (l + D + 1 < ncom) {
-            pf_so = P.asoff32[l + D + 1];
-            pf_sn = P.asoff32[l + D + 2] - pf_so;
-          }
-        }
+        if (l + D < ncom) stage_row(slot, P.vrow + (size_t)(l + D) * R, R, rank, nlive);
         cp_commit();
-      } else {
-        const uint32_t* vb = P.vrow + (size_t)l * R;
-        vi = rank_v(vb, vb + Wv, idx);
-        vf = rank_v(vb, vb + Wv, f);
-        vg = rank_v(vb, vb + Wv, g);
+        ri = (ri + 1 == D) ? 0 : ri + 1;
       }
       int nidx = al ? ref + vi : idx - vi;
       int nf = al ? ref + vf : f - vf;
@@ -466,9 +437,8 @@ __global__ void k_pbwt_union(PbwtSelectArgs a) {
 void launch_pbwt_select(const PbwtSelectArgs& a, cudaStream_t s) {
   k_pbwt_rng<<<1, 32, 0, s>>>(a);
   k_rare_carriers<<<dim3((a.Wc + 127) / 128, a.n_haps), 128, 0, s>>>(a);
-  // Ring of D slots (rank row + an index list of at most SEG entries), D <= 8, within 96 KB.
-  const int SEG = 256;
-  const size_t slot_bytes = ((size_t)a.P.R + SEG) * 4;
+  // Ring of D rank rows, D <= 8, within 96 KB.
+  const size_t slot_bytes = (size_t)a.P.R * 4;
   int D = (int)std::min<size_t>(8, (96u << 10) / slot_bytes);
   if (D < 2) D = 0;
   const size_t smem = (size_t)D * slot_bytes + 2 * 32 * 2 * 16 + (size_t)a.depth * 32 * 4;
@@ -477,7 +447,7 @@ void launch_pbwt_select(const PbwtSelectArgs& a, cudaStream_t s) {
     cudaFuncSetAttribute(k_pbwt_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 << 10);
     attr = true;
   }
-  k_pbwt_sweep<<<(a.n_haps + 31) / 32, 32, smem, s>>>(a, D, SEG);
+  k_pbwt_sweep<<<(a.n_haps + 31) / 32, 32, smem, s>>>(a, D);
   k_pbwt_union<<<(a.n_targets + 63) / 64, 64, 0, s>>>(a);
 }
 

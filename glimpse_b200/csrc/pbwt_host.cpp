@@ -214,7 +214,10 @@ int Context::pbwt_prepare_panel() {
   const int n_com_hq = host.n_com_hq;
   D.n_com_hq = n_com_hq;
   D.Wv = (N + 1 + 31) / 32;
-  D.R = (2 * D.Wv + 1 + 3) / 4 * 4;  // 16-byte rows, staged by the sweep with cp.async
+  // Row l: V bits and their prefix counts (select_common_pd_fg), then the bits and
+  // prefix counts of the small-PBWT positions merged at l (init_common); 16-byte
+  // rows, staged by the sweep with cp.async.
+  D.R = (4 * D.Wv + 2 + 3) / 4 * 4;
   const int Wv = D.Wv, R = D.R;
   cudaError_t e;
   if ((e = dev_alloc(&D.a_after, (size_t)n_com_hq * N, owned)) != cudaSuccess) return cuda_fail(e, "alloc pbwt");
@@ -302,6 +305,17 @@ int Context::pbwt_prepare_panel() {
       uint32_t* vp = vb + Wv;
       if (!decode(A, B, N, (int)host.cref[k], vb, vp, Wv))
         return (fail(GP_E_DATA, "sparse PBWT stream is malformed at site " + std::to_string(k)), GP_E_DATA);
+      {
+        uint32_t* sb = vb + 2 * Wv + 1;
+        uint32_t* sp = sb + Wv;
+        std::fill(sb, sb + 2 * Wv + 1, 0u);
+        if (initc[l_hq])
+          for (int64_t i = 0; i < sn; ++i) {
+            const int32_t q = sparse.asmall[so + i];
+            sb[q >> 5] |= 1u << (q & 31);
+          }
+        for (int w = 0; w < Wv; ++w) sp[w + 1] = sp[w] + (uint32_t)__builtin_popcount(sb[w]);
+      }
       std::copy(A.begin(), A.end(), stage_a.begin() + (size_t)stage_n * N);
       ++stage_n;
       site_info[k] = SK_COMMON | (l_hq << 2);
@@ -353,7 +367,7 @@ int Context::pbwt_prepare_panel() {
   {
     if (sparse.asmall_off.back() >= ((int64_t)1 << 31))
       return (fail(GP_E_DATA, "sparse PBWT: small-column index list exceeds 2^31 entries"), GP_E_DATA);
-    std::vector<int32_t> ev, aoff32(sparse.asmall_off.begin(), sparse.asmall_off.end());
+    std::vector<int32_t> ev;
     for (int k = 0; k < L; ++k) {
       if (host.lq[k]) continue;
       const int kind = site_info[k] & 3;
@@ -375,7 +389,6 @@ int Context::pbwt_prepare_panel() {
     int32_t* evd = nullptr;
     if ((e = dev_upload(&evd, ev, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");
     D.events = reinterpret_cast<int4*>(evd);
-    if ((e = dev_upload(&D.asoff32, aoff32, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");
   }
   if ((e = dev_upload(&D.init_common, initc, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");
   if ((e = dev_upload(&D.cm_pos, cmp, owned)) != cudaSuccess) return cuda_fail(e, "pbwt upload");

@@ -58,7 +58,6 @@ struct DevPbwt {
   //   run:    {k | 1 << 30, l, last site of the run, asoff[l]}, {sn(l), 0, 0, 0}
   int4* events = nullptr;
   int n_events = 0;
-  int32_t* asoff32 = nullptr;    // [n_com_hq + 2] asoff as int32
   uint8_t* init_common = nullptr;  // [n_com_hq]
   uint32_t* cref = nullptr;      // [L]
   float* cm_pos = nullptr;       // [L]  max(0, (float)cm)
