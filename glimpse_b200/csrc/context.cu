@@ -290,15 +290,19 @@ int Context::run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
   std::vector<int32_t> split(n);
   int64_t tot = 0;
   int Kmax = 0;
+  int Kall = 0;
+  for (int i = 0; i < n; ++i) Kall = std::max(Kall, host_nstates[i]);
+  w.Ks = impute_store_stride(Kall);
   for (int i = 0; i < n; ++i) {
     aoff[i] = tot;
-    tot += (int64_t)impute_np[i] * w.Kp;
+    tot += (int64_t)impute_np[i] * w.Ks;
     split[i] = (impute_np[i] / 2) & ~31;  // forward/backward meeting point, a multiple of 32
     Kmax = std::max(Kmax, host_nstates[i]);
   }
   if ((e = w.alpha.ensure((size_t)std::max<int64_t>(tot, 1) * 4)) != cudaSuccess) return cuda_fail(e, "alloc alpha");
   if ((e = w.split.ensure((size_t)n * 4)) != cudaSuccess) return cuda_fail(e, "alloc split");
-  if ((e = w.split_scr.ensure((size_t)n * (2 + w.Kp) * 4)) != cudaSuccess) return cuda_fail(e, "alloc split");
+  if ((e = w.split_scr.ensure(((size_t)((2 * n + 3) & ~3) + (size_t)n * w.Ks) * 4)) != cudaSuccess)
+    return cuda_fail(e, "alloc split");
   cudaMemcpyAsync(w.alpha_off.ptr, aoff.data(), n * 8, cudaMemcpyHostToDevice, stream);
   cudaMemcpyAsync(w.split.ptr, split.data(), n * 4, cudaMemcpyHostToDevice, stream);
   launch_site_records(panel, mc, w, d_hl, d_flat, stream);

@@ -47,8 +47,9 @@ struct StaticLayout {
 };
 
 // Upper bounds: the poly-site count is at most L (the exact count is known only
-// after compaction on the device), so the alpha store is sized L x Kp.
-StaticLayout static_layout(int L, int Kp) {
+// after compaction on the device), so the store is sized L x Ks (Ks: its row
+// stride in padded state coordinates).
+StaticLayout static_layout(int L, int Kp, int Ks) {
   const int WB = (L + 31) / 32;
   StaticLayout s{};
   size_t o = 0;
@@ -69,8 +70,8 @@ StaticLayout static_layout(int L, int Kp) {
   s.fl = take((size_t)L);
   s.alpha_off = take(8);
   s.split = take(4);
-  s.split_scr = take((size_t)(2 + Kp) * 4);
-  s.alpha = take((size_t)L * Kp * 4);
+  s.split_scr = take((size_t)(4 + Ks) * 4);
+  s.alpha = take((size_t)L * Ks * 4);
   s.hl = take((size_t)L * 2 * 4);
   s.hp = take((size_t)L * 2 * 4);
   s.flat = take((size_t)L);
@@ -102,7 +103,8 @@ extern "C" int gp_impute_one_static(gp_ctx* ctx, int32_t k, const uint32_t* stat
   }
   const int L = c.panel.L;
   const int Kp = (k + 31) / 32 * 32;
-  const gp::StaticLayout lay = gp::static_layout(L, Kp);
+  const int Ks = gp::impute_store_stride(k);
+  const gp::StaticLayout lay = gp::static_layout(L, Kp, Ks);
   if (lay.total > gp::kStaticScratchBytes)
     return (c.fail(GP_E_ARG, "impute_one_static: " + std::to_string(L) + " sites x " + std::to_string(k) +
                                  " states need " + std::to_string(lay.total >> 20) +
@@ -133,6 +135,7 @@ extern "C" int gp_impute_one_static(gp_ctx* ctx, int32_t k, const uint32_t* stat
   w.L = L;
   w.Kp = Kp;
   w.WB = (L + 31) / 32;
+  w.Ks = Ks;
   gp::point(w.states, base, lay.states, (size_t)Kp * 4);
   gp::point(w.nstates, base, lay.nstates, 4);
   gp::point(w.mark, base, lay.mark, L);
@@ -145,8 +148,8 @@ extern "C" int gp_impute_one_static(gp_ctx* ctx, int32_t k, const uint32_t* stat
   gp::point(w.fl, base, lay.fl, L);
   gp::point(w.alpha_off, base, lay.alpha_off, 8);
   gp::point(w.split, base, lay.split, 4);
-  gp::point(w.split_scr, base, lay.split_scr, (size_t)(2 + Kp) * 4);
-  gp::point(w.alpha, base, lay.alpha, (size_t)L * Kp * 4);
+  gp::point(w.split_scr, base, lay.split_scr, (size_t)(4 + Ks) * 4);
+  gp::point(w.alpha, base, lay.alpha, (size_t)L * Ks * 4);
   gp::point(w.hl, base, lay.hl, (size_t)L * 8);
   gp::point(w.hp, base, lay.hp, (size_t)L * 8);
   gp::point(w.flat, base, lay.flat, L);

@@ -65,6 +65,7 @@ struct DevPanel {
 // Per-batch scratch for the imputation path (sized for n haplotypes).
 struct ImputeWork {
   int n = 0, L = 0, Kp = 0, WB = 0;  // WB: 32-site blocks per haplotype (upper bound)
+  int Ks = 0;                         // row stride of the forward-backward store (padded state coordinates)
   DevBuf states, nstates, states_off;
   DevBuf mark, polyidx, poly, npoly;
   DevBuf hvar, em, tr, fl;
@@ -96,13 +97,12 @@ void launch_build_hvar(const DevPanel& P, ImputeWork& w, cudaStream_t s);
 void launch_site_records(const DevPanel& P, const ModelConst& mc, ImputeWork& w, const float* hl,
                          const uint8_t* flat, cudaStream_t s);
 int launch_impute_warp(int phase, int J, const ModelConst& mc, ImputeWork& w, float* hp, cudaStream_t s);
-// Register groups per lane of the imputation chain for at most Kmax states: the
-// groups in use, ((K + 31) / 32 rounded up to a multiple of 4), rounded up to
-// the next instantiated size (8, 16, ..., 64).
-inline int impute_groups(int Kmax) {
-  const int jn = (((Kmax + 31) / 32) + 3) & ~3;
-  return jn <= 8 ? 8 : (jn + 7) / 8 * 8;
-}
+// Register groups per lane of the imputation chain kernel for at most Kmax
+// states (the J of launch_impute_warp).
+int impute_groups(int Kmax);
+// Row stride (floats) of the forward-backward store for at most Kmax states; the
+// scratch split_scr holds round_up(2 n, 4) + n * stride floats.
+int impute_store_stride(int Kmax);
 void launch_impute_finish(const DevPanel& P, const ModelConst& mc, ImputeWork& w, const float* hl,
                         const uint8_t* flat, float* hp, cudaStream_t s);
 

@@ -1,14 +1,20 @@
-// Imputation HMM forward-backward with one warp per chain.
+// Imputation HMM forward-backward with W warps per chain and 4 states per lane
+// per quad.
 //
 // The haploid Li-Stephens recursion (phase/src/models/imputation_hmm.cpp:143-416)
-// is sequential over sites with a sum over all K states at every site. Here a
-// single warp runs one chain: lane `lane` owns states k = lane + 32 j (j < J),
-// the per-site sums are warp butterflies (no block barrier), and all memory
-// traffic is streamed ahead of the chain:
-//   * Hvar words of the next 32-site block and the stored rows of the next D
-//     sites go through a per-warp shared-memory ring filled by cp.async;
-//   * per-site records (emissions, transitions, flags) of the next block are
-//     loaded by the lanes one block ahead.
+// is sequential over sites with a sum over all K states at every site. A chain
+// (one haplotype in one direction) is run by W warps of one CTA. The states are
+// padded in front to 128 jq states (jq quads, a multiple of W) and warp w, lane
+// `lane`, local quad j owns the 4 consecutive padded states
+// 128 (W j + w) + 4 lane + c, c = 0..3 (state k = padded index - pad). Rows of
+// the store are kept in padded coordinates with stride Ks, so a lane's 4 values
+// of a row are one aligned 16-byte vector: phase 1 writes a row with one 16-byte
+// store per lane and quad, phase 2 stages rows with 16-byte cp.async. The
+// per-site sums are warp butterflies followed, for W > 1, by an exchange of the
+// W partial sums through shared memory behind a named barrier of the chain.
+// Hvar words of the next 32-site block and the stored rows of the next D sites
+// go through a per-warp shared-memory ring filled by cp.async; per-site records
+// (emissions, transitions, flags) of the next block are loaded one block ahead.
 //
 // Each haplotype is split at M (a multiple of 32) into two chains that run
 // concurrently and meet in the middle (no waiting between them):
@@ -20,9 +26,10 @@
 // Rows [0, M) of the store hold alpha and rows [M, np) prob_curr: one 4-byte
 // write and one read per (site, state), plus 1/8 byte of Hvar per pass.
 //
-// Sums follow a fixed order (lane-sequential over j, then a lane butterfly), so
-// results are deterministic. Every fused multiply-add is an explicit fmaf where
-// the reference's compiled arithmetic has one (build with --fmad=false).
+// Sums follow a fixed order (per lane over quads and components, then a lane
+// butterfly, then the warps in order), so results are deterministic. Every fused
+// multiply-add is an explicit fmaf where the reference's compiled arithmetic has
+// one (build with --fmad=false).
 #include <type_traits>
 
 #include "internal.h"
@@ -31,12 +38,16 @@ namespace gp {
 
 namespace {
 
-constexpr int kWarpsPerCta = 2;
-constexpr int kRowDepth = 3;              // stored rows fetched this many sites ahead
+constexpr int kChainsPerCta = 2;
+constexpr int kWarpsPerChain = 1;       // W
+constexpr int kRowDepth = 3;         // stored rows fetched this many sites ahead
 constexpr int kRing = kRowDepth + 1;      // ring slots
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_addr(smem)), "l"(gmem));
 }
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(smem)), "l"(gmem));
@@ -45,18 +56,6 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
-
-// Copy Kp 4-byte values (Kp a multiple of 32, at most 32 * J, 16-byte aligned)
-// into shared memory: 16-byte chunk lane + 32 c for c < J / 4.
-template <int J>
-__device__ __forceinline__ void copy_row_async(void* dst, const void* src, int Kp, int lane) {
-  const int chunks = Kp >> 2;
-  const char* s = static_cast<const char*>(src) + 16 * lane;
-  char* d = static_cast<char*>(dst) + 16 * lane;
-#pragma unroll
-  for (int c = 0; c < J / 4; ++c)
-    if (lane + 32 * c < chunks) cp_async16(d + 512 * c, s + 512 * c);
 }
 
 __device__ __forceinline__ float warp_sum(float v) {
@@ -68,36 +67,66 @@ __device__ __forceinline__ float warp_sum(float v) {
 struct WarpScratch {
   float* asum;          // [n] AlphaSum at site M-1
   float* bsum;          // [n] betaSum at site M
-  float* brow;          // [n][Kp] Beta at site M
+  float* brow;          // [n][Ks] Beta at site M, padded coordinates
   const int32_t* split; // [n] M
 };
 
-// Per-warp shared memory: records (2 blocks), Hvar words (2 blocks), row ring.
+// Per-warp shared memory: records (2 blocks), Hvar words (2 blocks) and a row
+// ring, both holding the warp's own states: [buffer][quad j][lane] x 16 bytes.
 struct WarpSmem {
-  float4* em;     // [2][32]
-  float2* tr;     // [2][32]
-  int32_t* pl;    // [2][32] site of the poly index
-  uint8_t* fl;    // [2][32]
-  uint32_t* words;  // [2][Kp]
-  float* ring;    // [kRing][Kp]
+  float4* em;       // [2][32]
+  float2* tr;       // [2][32]
+  int32_t* pl;      // [2][32] site of the poly index
+  uint4* words;     // [2][J][32]
+  float4* ring;     // [kRing][J][32]
+  uint8_t* fl;      // [2][32]
 };
 
-__device__ __forceinline__ WarpSmem carve(char* base, int Kp) {
+__host__ __device__ __forceinline__ size_t warp_smem_bytes(int J) {
+  return 2 * 32 * 16 + 2 * 32 * 8 + 2 * 32 * 4 + (size_t)(2 + kRing) * J * 32 * 16 + 2 * 32;
+}
+
+__device__ __forceinline__ WarpSmem carve(char* base, int J) {
   WarpSmem m;
-  m.em = reinterpret_cast<float4*>(base);
-  m.tr = reinterpret_cast<float2*>(base + 2 * 32 * 16);
-  m.words = reinterpret_cast<uint32_t*>(base + 2 * 32 * 16 + 2 * 32 * 8);
-  m.ring = reinterpret_cast<float*>(base + 2 * 32 * 16 + 2 * 32 * 8 + 2 * (size_t)Kp * 4);
-  m.pl = reinterpret_cast<int32_t*>(base + 2 * 32 * 16 + 2 * 32 * 8 + 2 * (size_t)Kp * 4 +
-                                    (size_t)kRing * Kp * 4);
-  m.fl = reinterpret_cast<uint8_t*>(base + 2 * 32 * 16 + 2 * 32 * 8 + 2 * (size_t)Kp * 4 +
-                                    (size_t)kRing * Kp * 4 + 2 * 32 * 4);
+  size_t o = 0;
+  m.em = reinterpret_cast<float4*>(base + o);
+  o += 2 * 32 * 16;
+  m.tr = reinterpret_cast<float2*>(base + o);
+  o += 2 * 32 * 8;
+  m.pl = reinterpret_cast<int32_t*>(base + o);
+  o += 2 * 32 * 4;
+  m.words = reinterpret_cast<uint4*>(base + o);
+  o += (size_t)2 * J * 32 * 16;
+  m.ring = reinterpret_cast<float4*>(base + o);
+  o += (size_t)kRing * J * 32 * 16;
+  m.fl = reinterpret_cast<uint8_t*>(base + o);
   return m;
 }
 
-__host__ __device__ __forceinline__ size_t warp_smem_bytes(int Kp) {
-  return 2 * 32 * 16 + 2 * 32 * 8 + 2 * (size_t)Kp * 4 + (size_t)kRing * Kp * 4 + 2 * 32 * 4 + 2 * 32 + 64;
+// Sum over the W warps of a chain of each warp's partial sums (x, y, z), in
+// warp order, through a double-buffered exchange slot and a named barrier of
+// the chain's 32 W threads.
+template <int W>
+__device__ __forceinline__ float3 chain_sum(float x, float y, float z, float4* xch, int parity, int wi, int lane,
+                                            int bar_id) {
+  if (W == 1) return make_float3(x, y, z);
+  float4* slot = xch + parity * W;
+  if (lane == 0) slot[wi] = make_float4(x, y, z, 0.f);
+  asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(32 * W) : "memory");
+  float4 s = slot[0];
+#pragma unroll
+  for (int i = 1; i < W; ++i) {
+    const float4 v = slot[i];
+    s.x = __fadd_rn(s.x, v.x);
+    s.y = __fadd_rn(s.y, v.y);
+    s.z = __fadd_rn(s.z, v.z);
+  }
+  return make_float3(s.x, s.y, s.z);
 }
+
+__device__ __forceinline__ float& comp(float4& v, int c) { return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w; }
+__device__ __forceinline__ uint32_t compu(const uint4& v, int c) { return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w; }
+__device__ __forceinline__ float compf(const float4& v, int c) { return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w; }
 
 // One site of a chain for the owned states, specialised at compile time:
 //   FWD   forward (alpha) or backward (Beta) recursion
@@ -107,54 +136,43 @@ __host__ __device__ __forceinline__ size_t warp_smem_bytes(int Kp) {
 // so the same loop serves both kinds of site.
 // At the last site the forward posterior uses alpha alone and the stored
 // prob_curr is 1 there, so alpha x 1 is used unchanged (imputation_hmm.cpp:337-368).
-// m selects the current site's bit in the Hvar words; rowl / srowl point at this
-// lane's state of group 0 in the staged row (shared) and in the stored row
-// (global), so group j is at offset 32 j. Padded lanes of groups 0..3 never
-// dereference them.
-template <int J, bool FWD, bool POST, bool INIT>
-__device__ __forceinline__ void chain_step(float (&x)[J], const uint32_t (&w)[J], uint32_t m, float (&q0)[4],
-                                           float (&q1)[4], float (&q2)[4], const bool (&vg)[4], int jn, float fact1,
-                                           float fact2, float ex, float ey, const float* rowl, float* srowl) {
+// m selects the current site's bit in the Hvar words; rowl points at this lane's
+// staged row vector of local quad 0 (shared, quad j at offset 32 j) and srowl at
+// its stored row vector (global, quad j at offset 32 W j). Padded states
+// (quad 0 only) are kept at 0; the vectors are written whole.
+template <int J, int W, bool FWD, bool POST, bool INIT>
+__device__ __forceinline__ void chain_step(float4 (&x)[J], const uint4 (&w)[J], uint32_t m, float (&q0)[4],
+                                           float (&q1)[4], float (&q2)[4], const bool (&vq)[4], int G, float fact1,
+                                           float fact2, float ex, float ey, const float4* rowl, float4* srowl) {
 #pragma unroll
-  for (int j0 = 0; j0 < J; j0 += 4) {
-    if (j0 >= jn) break;  // jn is the same on every lane
-    {
+  for (int j = 0; j < J; ++j) {
+    if (j >= G) break;  // G is the same on every lane
+    float4 r4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (POST) r4 = rowl[32 * j];
+    float4 st;
 #pragma unroll
-      for (int jj = 0; jj < 4; ++jj) {
-        const int j = j0 + jj;
-        const bool valid = j >= 4 || vg[jj];
-        const bool bit = (w[j] & m) != 0u;
-        const float pcv = INIT ? fact1 : fmaf(x[j], fact2, fact1);
-        float nx = __fmul_rn(pcv, bit ? ey : ex);
-        if (j < 4) nx = valid ? nx : 0.f;
-        x[j] = nx;
-        q0[jj] = __fadd_rn(q0[jj], nx);
-        if (POST) {
-          float r = 0.f;
-          if (valid) r = rowl[32 * j];
-          float d;
-          if (FWD) d = __fmul_rn(nx, r);           // alpha x stored prob_curr (1 at the last site)
-          else d = INIT ? r : __fmul_rn(r, pcv);  // stored alpha x prob_curr; alpha alone at the last site
-          if (bit) q2[jj] = __fadd_rn(q2[jj], d);
-          else q1[jj] = __fadd_rn(q1[jj], d);
-        } else if (valid) {
-          srowl[32 * j] = FWD ? nx : (INIT ? 1.0f : pcv);
-        }
+    for (int c = 0; c < 4; ++c) {
+      const bool bit = (compu(w[j], c) & m) != 0u;
+      const float pcv = INIT ? fact1 : fmaf(compf(x[j], c), fact2, fact1);
+      float nx = __fmul_rn(pcv, bit ? ey : ex);
+      if (j == 0) nx = vq[c] ? nx : 0.f;
+      comp(x[j], c) = nx;
+      q0[c] = __fadd_rn(q0[c], nx);
+      if (POST) {
+        const float r = compf(r4, c);
+        float d;
+        if (FWD) d = __fmul_rn(nx, r);           // alpha x stored prob_curr (1 at the last site)
+        else d = INIT ? r : __fmul_rn(r, pcv);  // stored alpha x prob_curr; alpha alone at the last site
+        if (bit) q2[c] = __fadd_rn(q2[c], d);
+        else q1[c] = __fadd_rn(q1[c], d);
+      } else {
+        comp(st, c) = FWD ? nx : (INIT ? 1.0f : pcv);
       }
     }
+    if (!POST) srowl[32 * W * j] = st;
   }
 }
 
-// State layout inside a chain: the K states are padded to 32 * jn states with
-// jn a multiple of 4, and the padding is put in front: lane `lane` of group j
-// holds state k = 32 j + lane - pad (pad = 32 jn - K < 128). Only groups 0..3
-// contain padding, so only they carry validity masks; padded states are kept at
-// exactly 0 and therefore add nothing to any sum. Groups are processed in
-// chunks of 4 behind one warp-uniform branch, so a chain's work follows its own K.
-//
-// Site bits: the 32-bit Hvar word of a state covers a 32-site block; it is kept
-// shifted so that the current site's bit is the sign bit (bit-reversed for the
-// forward direction), which turns the emission choice into a sign test.
 // Arguments of one launch, shared by the forward and backward chains.
 struct ChainArgs {
   int nchains;
@@ -168,17 +186,41 @@ struct ChainArgs {
   const int64_t* __restrict__ store_off;
   float* __restrict__ store_pool;
   WarpScratch sc;
-  int L, WB, Kp;
+  int L, WB, Kp, Ks;
   ModelConst mc;
   float* __restrict__ hp;
 };
 
-// One chain (a haplotype in one direction) over its sites [lo, hi), with the
-// direction FWD and the phase (POST = phase 2) fixed at compile time, so the
-// per-site loop carries no dispatch. The first site of a chain is peeled when it
-// starts the recursion (INIT).
-template <int J, bool FWD, bool POST>
-__device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, int t, int lane) {
+// Hvar words of this lane's states (state index kb + 128 W j + c) of one block
+// row, into dst[32 j] (dst already offset by the lane); padded states skipped.
+template <int J, int W>
+__device__ __forceinline__ void fetch_words(uint4* dst, const uint32_t* row, int kb, int G) {
+#pragma unroll
+  for (int j = 0; j < J; ++j) {
+    if (j >= G) break;
+    uint32_t* d = reinterpret_cast<uint32_t*>(dst + 32 * j);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int k = kb + 128 * W * j + c;
+      if (k >= 0) cp_async4(d + c, row + k);
+    }
+  }
+}
+
+// This lane's vectors of a stored row (padded coordinates; quad j at vector
+// offset 32 W j from the lane's quad 0) into dst[32 j].
+template <int J, int W>
+__device__ __forceinline__ void fetch_row(float4* dst, const float4* rowl, int G) {
+#pragma unroll
+  for (int j = 0; j < J; ++j) {
+    if (j >= G) break;
+    cp_async16(dst + 32 * j, rowl + 32 * W * j);
+  }
+}
+
+template <int J, int W, bool FWD, bool POST>
+__device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, float4* xch, int t, int wi, int lane,
+                                          int bar_id) {
   const int np = A.npoly[t];
   const int K = A.nstates[t];
   const int M = A.sc.split[t];
@@ -186,14 +228,16 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, int t,
   const int lo = (FWD == POST) ? M : 0;   // phase 1: forward [0, M), backward [M, np)
   const int hi = (FWD == POST) ? np : M;  // phase 2: forward [M, np), backward [0, M)
   if (lo >= hi) return;
-  const int Kp = A.Kp;
-  const int jn = (((K + 31) >> 5) + 3) & ~3;  // groups in use, a multiple of 4
-  const int pad = 32 * jn - K;
-  bool vg[4];                                 // validity of this lane in groups 0..3
+  const int Kp = A.Kp, Ks = A.Ks;
+  const int jq = ((K + 127) / 128 + W - 1) / W * W;  // quads, a multiple of W
+  const int G = jq / W;                               // local quads
+  const int pad = 128 * jq - K;                       // < 128 W: only global quads < W (local quad 0) are padded
+  const int pb = 128 * wi + 4 * lane;                 // padded index of this lane's quad 0
+  const int kb = pb - pad;                            // its state index
+  bool vq[4];
 #pragma unroll
-  for (int j = 0; j < 4; ++j) vg[j] = (32 * j + lane) >= pad;
-  const int kb = lane - pad;                  // state index of group 0 for this lane
-  WarpSmem S = carve(smem, Kp);
+  for (int c = 0; c < 4; ++c) vq[c] = pb + c >= pad;
+  WarpSmem S = carve(smem, J);
   float* store = A.store_pool + A.store_off[t];
   const uint32_t* hv = A.hvar + (size_t)t * A.WB * Kp;
   const float4* E = A.em + (size_t)t * A.L;
@@ -204,9 +248,10 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, int t,
   const int n = hi - lo;
   const float Kf = (float)K;
   auto site_of = [&](int s) { return FWD ? lo + s : hi - 1 - s; };
-  // index of the value owned by (j, lane) in a K-long row; padding reads entry 0
-  auto idx = [&](int j) { return max(32 * j + kb, 0); };
+  auto row_vec = [&](int l) { return reinterpret_cast<float4*>(store + (size_t)l * Ks + pb); };
   constexpr int dir = FWD ? 1 : -1;
+  uint4* wl = S.words + lane;   // this lane's words; block buffer (b & 1) at offset 32 J (b & 1)
+  float4* rl = S.ring + lane;   // this lane's staged row vectors; slot s at offset 32 J s
 
   // ---- prologue: records and Hvar words of the first two blocks, first rows ----
   const int b_first = site_of(0) >> 5;
@@ -219,41 +264,43 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, int t,
       S.fl[(b_first & 1) * 32 + lane] = F[l];
       S.pl[(b_first & 1) * 32 + lane] = PL[l];
     }
-    copy_row_async<J>(S.words + (size_t)(b_first & 1) * Kp, hv + (size_t)b_first * Kp, Kp, lane);
+    fetch_words<J, W>(wl + (b_first & 1) * 32 * J, hv + (size_t)b_first * Kp, kb, G);
     if (b_first != b_last) {
       const int b2 = b_first + dir;
-      copy_row_async<J>(S.words + (size_t)(b2 & 1) * Kp, hv + (size_t)b2 * Kp, Kp, lane);
+      fetch_words<J, W>(wl + (b2 & 1) * 32 * J, hv + (size_t)b2 * Kp, kb, G);
     }
   }
   cp_commit();
   if (POST) {
 #pragma unroll
     for (int d = 0; d < kRowDepth; ++d) {
-      if (d < n) copy_row_async<J>(S.ring + (size_t)(d % kRing) * Kp, store + (size_t)site_of(d) * Kp, Kp, lane);
+      if (d < n) fetch_row<J, W>(rl + (d % kRing) * 32 * J, row_vec(site_of(d)), G);
       cp_commit();
     }
   }
 
-  float x[J];      // alpha (forward) or Beta (backward)
-  uint32_t w[J];   // Hvar words of the current block
+  float4 x[J];  // alpha (forward) or Beta (backward)
+  uint4 w[J];   // Hvar words of the current block
 #pragma unroll
   for (int j = 0; j < J; ++j) {
-    x[j] = 0.f;
-    w[j] = 0u;
+    x[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+    w[j] = make_uint4(0u, 0u, 0u, 0u);
   }
   float acc = 0.f;  // AlphaSum / betaSum of the previous step
   float2 t_prev = make_float2(0.f, 0.f);
   if (FWD && lo > 0) {
+    const float4* r = row_vec(lo - 1);
 #pragma unroll
     for (int j = 0; j < J; ++j)
-      if (j < jn) x[j] = (j >= 4 || vg[j & 3]) ? store[(size_t)(lo - 1) * Kp + idx(j)] : 0.f;
+      if (j < G) x[j] = r[32 * W * j];
     acc = A.sc.asum[t];
     t_prev = T[lo - 1];
   }
   if (!FWD && hi < np) {
+    const float4* r = reinterpret_cast<const float4*>(A.sc.brow + (size_t)t * Ks + pb);
 #pragma unroll
     for (int j = 0; j < J; ++j)
-      if (j < jn) x[j] = (j >= 4 || vg[j & 3]) ? A.sc.brow[(size_t)t * Kp + idx(j)] : 0.f;
+      if (j < G) x[j] = r[32 * W * j];
     acc = A.sc.bsum[t];
   }
   float4 pe = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -283,7 +330,7 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, int t,
         const int bn = b + dir;
         const int ln = (bn << 5) + lane;
         if (ln < np) { pe = E[ln]; pt = T[ln]; pf = F[ln]; pp = PL[ln]; }
-        copy_row_async<J>(S.words + (size_t)(bn & 1) * Kp, hv + (size_t)bn * Kp, Kp, lane);
+        fetch_words<J, W>(wl + (bn & 1) * 32 * J, hv + (size_t)bn * Kp, kb, G);
       }
       if (!POST) {
         cp_commit();
@@ -291,24 +338,22 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, int t,
       }
     }
     if (POST) {
-      if (s + kRowDepth < n)
-        copy_row_async<J>(S.ring + (size_t)((s + kRowDepth) % kRing) * Kp,
-                          store + (size_t)site_of(s + kRowDepth) * Kp, Kp, lane);
+      if (s + kRowDepth < n) fetch_row<J, W>(rl + ((s + kRowDepth) % kRing) * 32 * J, row_vec(site_of(s + kRowDepth)), G);
       cp_commit();
       cp_wait<kRowDepth>();
     }
     __syncwarp();
     if (new_block) {
-      const uint32_t* wbl = S.words + (size_t)(b & 1) * Kp + kb;
+      const uint4* wb = wl + (b & 1) * 32 * J;
 #pragma unroll
       for (int j = 0; j < J; ++j)
-        if (j < jn) w[j] = (j >= 4 || vg[j & 3]) ? wbl[32 * j] : 0u;
+        if (j < G) w[j] = wb[32 * j];
     }
     const uint32_t m = 1u << i;
     const uint8_t f = S.fl[(b & 1) * 32 + i];
     const float4 e = S.em[(b & 1) * 32 + i];
-    const float* rowl = S.ring + (size_t)(s % kRing) * Kp + kb;
-    float* srowl = store + (size_t)l * Kp + kb;
+    const float4* rowl = rl + (s % kRing) * 32 * J;
+    float4* srowl = row_vec(l);
     float q0[4] = {0.f, 0.f, 0.f, 0.f}, q1[4] = {0.f, 0.f, 0.f, 0.f}, q2[4] = {0.f, 0.f, 0.f, 0.f};
     float fact1, fact2;
     if (INIT) {
@@ -323,17 +368,20 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, int t,
       fact2 = tt.y / acc;
     }
     const float ex = f ? 1.0f : e.x, ey = f ? 1.0f : e.y;
-    chain_step<J, FWD, POST, INIT>(x, w, m, q0, q1, q2, vg, jn, fact1, fact2, ex, ey, rowl, srowl);
+    chain_step<J, W, FWD, POST, INIT>(x, w, m, q0, q1, q2, vq, G, fact1, fact2, ex, ey, rowl, srowl);
     const float v0 = warp_sum(__fadd_rn(__fadd_rn(q0[0], q0[1]), __fadd_rn(q0[2], q0[3])));
-    // AlphaSum = 1 at a flat first site, betaSum = 1 at a flat last site (imputation_hmm.cpp:156,285)
-    acc = (INIT && f) ? 1.0f : v0;
-    if (FWD) t_prev = S.tr[(b & 1) * 32 + i];
+    float v1 = 0.f, v2 = 0.f;
     if (POST) {
-      const float v1 = warp_sum(__fadd_rn(__fadd_rn(q1[0], q1[1]), __fadd_rn(q1[2], q1[3])));
-      const float v2 = warp_sum(__fadd_rn(__fadd_rn(q2[0], q2[1]), __fadd_rn(q2[2], q2[3])));
-      // prob_hid of the two alleles; k_impute_finish turns them into HP
-      if (lane == 0) *reinterpret_cast<float2*>(HP + 2 * S.pl[(b & 1) * 32 + i]) = make_float2(v1, v2);
+      v1 = warp_sum(__fadd_rn(__fadd_rn(q1[0], q1[1]), __fadd_rn(q1[2], q1[3])));
+      v2 = warp_sum(__fadd_rn(__fadd_rn(q2[0], q2[1]), __fadd_rn(q2[2], q2[3])));
     }
+    const float3 tot = chain_sum<W>(v0, v1, v2, xch, s & 1, wi, lane, bar_id);
+    // AlphaSum = 1 at a flat first site, betaSum = 1 at a flat last site (imputation_hmm.cpp:156,285)
+    acc = (INIT && f) ? 1.0f : tot.x;
+    if (FWD) t_prev = S.tr[(b & 1) * 32 + i];
+    // prob_hid of the two alleles; k_impute_finish turns them into HP
+    if (POST && wi == 0 && lane == 0)
+      *reinterpret_cast<float2*>(HP + 2 * S.pl[(b & 1) * 32 + i]) = make_float2(tot.y, tot.z);
     __syncwarp();
   };
 
@@ -349,50 +397,73 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, int t,
   cp_wait<0>();
   if (!POST) {
     if (FWD) {
-      if (lane == 0) A.sc.asum[t] = acc;
+      if (wi == 0 && lane == 0) A.sc.asum[t] = acc;
     } else {
+      float4* r = reinterpret_cast<float4*>(A.sc.brow + (size_t)t * Ks + pb);
 #pragma unroll
       for (int j = 0; j < J; ++j)
-        if (j < jn && (j >= 4 || vg[j & 3])) A.sc.brow[(size_t)t * Kp + idx(j)] = x[j];
-      if (lane == 0) A.sc.bsum[t] = acc;
+        if (j < G) r[32 * W * j] = x[j];
+      if (wi == 0 && lane == 0) A.sc.bsum[t] = acc;
     }
   }
 }
 
-// Warp `warp` of the CTA runs chain blockIdx.x * kWarpsPerCta + warp: target
-// chain / 2, forward for even chains and backward for odd ones.
-template <int J, bool POST>
-__global__ void __launch_bounds__(32 * kWarpsPerCta) k_impute_warp(ChainArgs A) {
-  static_assert(J % 4 == 0, "groups are processed in chunks of 4");
+// Chain c = blockIdx.x * kChainsPerCta + (warp / W) is run by the W warps
+// (warp % W = 0..W-1) of its slot: target c / 2, forward for even chains and
+// backward for odd ones. Every warp of a chain takes the same branches, so the
+// chain's named barrier (id 1 + slot) always sees all 32 W threads.
+template <int J, int W, bool POST>
+__global__ void __launch_bounds__(32 * W * kChainsPerCta) k_impute_warp(ChainArgs A) {
   extern __shared__ __align__(16) char smem_raw[];
+  __shared__ float4 xch[kChainsPerCta][2 * W];
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  const int chain = blockIdx.x * kWarpsPerCta + warp;
+  const int slot = warp / W, wi = warp % W;
+  const int chain = blockIdx.x * kChainsPerCta + slot;
   if (chain >= A.nchains) return;
-  char* smem = smem_raw + (size_t)warp * warp_smem_bytes(A.Kp);
-  if ((chain & 1) == 0) run_chain<J, true, POST>(A, smem, chain >> 1, lane);
-  else run_chain<J, false, POST>(A, smem, chain >> 1, lane);
+  char* smem = smem_raw + (size_t)warp * warp_smem_bytes(J);
+  if ((chain & 1) == 0) run_chain<J, W, true, POST>(A, smem, xch[slot], chain >> 1, wi, lane, 1 + slot);
+  else run_chain<J, W, false, POST>(A, smem, xch[slot], chain >> 1, wi, lane, 1 + slot);
 }
 
 }  // namespace
 
-size_t impute_warp_smem(int Kp) { return (size_t)kWarpsPerCta * warp_smem_bytes(Kp); }
+size_t impute_warp_smem(int J) { return (size_t)kWarpsPerChain * kChainsPerCta * warp_smem_bytes(J); }
+
+// Local quads per warp for at most Kmax states (the J of launch_impute_warp).
+int impute_groups(int Kmax) {
+  const int W = kWarpsPerChain;
+  const int jq = ((Kmax + 127) / 128 + W - 1) / W * W;
+  const int G = jq / W;
+  return G <= 2 ? 2 : (G <= 4 ? 4 : (G + 3) / 4 * 4);
+}
+
+// Row stride of the store in padded coordinates for at most Kmax states.
+int impute_store_stride(int Kmax) {
+  const int W = kWarpsPerChain;
+  return 128 * (((Kmax + 127) / 128 + W - 1) / W * W);
+}
 
 template <int J, bool POST>
-static void launch_chains(const ChainArgs& a, dim3 g, size_t sm, cudaStream_t s) {
+static int launch_chains(const ChainArgs& a, cudaStream_t s) {
+  constexpr int W = kWarpsPerChain;
+  const size_t sm = impute_warp_smem(J);
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_impute_warp<J, POST>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_impute_warp<J, W, POST>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
   }
-  k_impute_warp<J, POST><<<g, 32 * kWarpsPerCta, sm, s>>>(a);
+  if (sm > 200 * 1024) return GP_E_ARG;
+  const dim3 g((a.nchains + kChainsPerCta - 1) / kChainsPerCta);
+  k_impute_warp<J, W, POST><<<g, 32 * W * kChainsPerCta, sm, s>>>(a);
+  return GP_OK;
 }
 
 int launch_impute_warp(int phase, int J, const ModelConst& mc, ImputeWork& w, float* hp, cudaStream_t s) {
   ChainArgs a;
   a.sc.asum = w.split_scr.as<float>();
   a.sc.bsum = a.sc.asum + w.n;
-  a.sc.brow = a.sc.bsum + w.n;
+  a.sc.brow = a.sc.asum + ((2 * w.n + 3) & ~3);  // 16-byte aligned rows of Ks floats
   a.sc.split = w.split.as<int32_t>();
   a.nchains = 2 * w.n;
   a.poly = w.poly.as<int32_t>();
@@ -407,21 +478,16 @@ int launch_impute_warp(int phase, int J, const ModelConst& mc, ImputeWork& w, fl
   a.L = w.L;
   a.WB = w.WB;
   a.Kp = w.Kp;
+  a.Ks = w.Ks;
   a.mc = mc;
   a.hp = hp;
-  const dim3 g((a.nchains + kWarpsPerCta - 1) / kWarpsPerCta);
-  const size_t sm = impute_warp_smem(w.Kp);
-#define GP_WARP(JJ)                                                           \
-  case JJ:                                                                    \
-    if (phase == 2) launch_chains<JJ, true>(a, g, sm, s);                     \
-    else launch_chains<JJ, false>(a, g, sm, s);                               \
-    break;
+#define GP_WARP(JJ) \
+  case JJ: return phase == 2 ? launch_chains<JJ, true>(a, s) : launch_chains<JJ, false>(a, s);
   switch (J) {
-    GP_WARP(8) GP_WARP(16) GP_WARP(24) GP_WARP(32) GP_WARP(40) GP_WARP(48) GP_WARP(56) GP_WARP(64)
+    GP_WARP(2) GP_WARP(4) GP_WARP(8) GP_WARP(12) GP_WARP(16)
     default: return GP_E_ARG;
   }
 #undef GP_WARP
-  return GP_OK;
 }
 
 }  // namespace gp
