@@ -4,9 +4,11 @@
 // The haploid Li-Stephens recursion (phase/src/models/imputation_hmm.cpp:143-416)
 // is sequential over sites with a sum over all K states at every site. A chain
 // (one haplotype in one direction) is run by W warps of one CTA. The states are
-// padded in front to 128 jq states (jq quads, a multiple of W) and warp w, lane
-// `lane`, local quad j owns the 4 consecutive padded states
-// 128 (W j + w) + 4 lane + c, c = 0..3 (state k = padded index - pad). Rows of
+// padded in front to the launch's 128 W J states (J quads per warp, from the
+// largest K of the call) and warp w, lane `lane`, local quad j owns the 4
+// consecutive padded states 128 (W j + w) + 4 lane + c, c = 0..3 (state k =
+// padded index - pad). Every chain runs all J quads, so a site is one
+// straight-line block for the scheduler; padded states are held at 0. Rows of
 // the store are kept in padded coordinates with stride Ks, so a lane's 4 values
 // of a row are one aligned 16-byte vector: phase 1 writes a row with one 16-byte
 // store per lane and quad, phase 2 stages rows with 16-byte cp.async. The
@@ -30,6 +32,7 @@
 // butterfly, then the warps in order), so results are deterministic. Every fused
 // multiply-add is an explicit fmaf where the reference's compiled arithmetic has
 // one (build with --fmad=false).
+#include <algorithm>
 #include <type_traits>
 
 #include "internal.h"
@@ -138,15 +141,15 @@ __device__ __forceinline__ float compf(const float4& v, int c) { return c == 0 ?
 // prob_curr is 1 there, so alpha x 1 is used unchanged (imputation_hmm.cpp:337-368).
 // m selects the current site's bit in the Hvar words; rowl points at this lane's
 // staged row vector of local quad 0 (shared, quad j at offset 32 j) and srowl at
-// its stored row vector (global, quad j at offset 32 W j). Padded states
-// (quad 0 only) are kept at 0; the vectors are written whole.
+// its stored row vector (global, quad j at offset 32 W j). Every chain of a
+// launch runs the launch's J quads, so a site is one straight-line block; the
+// padded states (vf = 0) are kept at 0, and the vectors are written whole.
 template <int J, int W, bool FWD, bool POST, bool INIT>
 __device__ __forceinline__ void chain_step(float4 (&x)[J], const uint4 (&w)[J], uint32_t m, float (&q0)[4],
-                                           float (&q1)[4], float (&q2)[4], const bool (&vq)[4], int G, float fact1,
+                                           float (&q1)[4], float (&q2)[4], const float4 (&vf)[J], float fact1,
                                            float fact2, float ex, float ey, const float4* rowl, float4* srowl) {
 #pragma unroll
   for (int j = 0; j < J; ++j) {
-    if (j >= G) break;  // G is the same on every lane
     float4 r4 = make_float4(0.f, 0.f, 0.f, 0.f);
     if (POST) r4 = rowl[32 * j];
     float4 st;
@@ -154,8 +157,8 @@ __device__ __forceinline__ void chain_step(float4 (&x)[J], const uint4 (&w)[J], 
     for (int c = 0; c < 4; ++c) {
       const bool bit = (compu(w[j], c) & m) != 0u;
       const float pcv = INIT ? fact1 : fmaf(compf(x[j], c), fact2, fact1);
-      float nx = __fmul_rn(pcv, bit ? ey : ex);
-      if (j == 0) nx = vq[c] ? nx : 0.f;
+      // padded states are multiplied by 0, valid ones by 1 (exact)
+      const float nx = __fmul_rn(__fmul_rn(pcv, bit ? ey : ex), compf(vf[j], c));
       comp(x[j], c) = nx;
       q0[c] = __fadd_rn(q0[c], nx);
       if (POST) {
@@ -194,10 +197,9 @@ struct ChainArgs {
 // Hvar words of this lane's states (state index kb + 128 W j + c) of one block
 // row, into dst[32 j] (dst already offset by the lane); padded states skipped.
 template <int J, int W>
-__device__ __forceinline__ void fetch_words(uint4* dst, const uint32_t* row, int kb, int G) {
+__device__ __forceinline__ void fetch_words(uint4* dst, const uint32_t* row, int kb) {
 #pragma unroll
   for (int j = 0; j < J; ++j) {
-    if (j >= G) break;
     uint32_t* d = reinterpret_cast<uint32_t*>(dst + 32 * j);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
@@ -210,10 +212,9 @@ __device__ __forceinline__ void fetch_words(uint4* dst, const uint32_t* row, int
 // This lane's vectors of a stored row (padded coordinates; quad j at vector
 // offset 32 W j from the lane's quad 0) into dst[32 j].
 template <int J, int W>
-__device__ __forceinline__ void fetch_row(float4* dst, const float4* rowl, int G) {
+__device__ __forceinline__ void fetch_row(float4* dst, const float4* rowl) {
 #pragma unroll
   for (int j = 0; j < J; ++j) {
-    if (j >= G) break;
     cp_async16(dst + 32 * j, rowl + 32 * W * j);
   }
 }
@@ -229,14 +230,16 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, float4
   const int hi = (FWD == POST) ? np : M;  // phase 2: forward [M, np), backward [0, M)
   if (lo >= hi) return;
   const int Kp = A.Kp, Ks = A.Ks;
-  const int jq = ((K + 127) / 128 + W - 1) / W * W;  // quads, a multiple of W
-  const int G = jq / W;                               // local quads
-  const int pad = 128 * jq - K;                       // < 128 W: only global quads < W (local quad 0) are padded
-  const int pb = 128 * wi + 4 * lane;                 // padded index of this lane's quad 0
-  const int kb = pb - pad;                            // its state index
-  bool vq[4];
+  const int pad = 128 * W * J - K;    // every chain is padded in front to the launch's 128 W J states
+  const int pb = 128 * wi + 4 * lane;  // padded index of this lane's quad 0
+  const int kb = pb - pad;             // its state index
+  float4 vf[J];                        // 1 for a state, 0 for padding
 #pragma unroll
-  for (int c = 0; c < 4; ++c) vq[c] = pb + c >= pad;
+  for (int j = 0; j < J; ++j) {
+    const int q = pb + 128 * W * j;
+    vf[j] = make_float4(q >= pad ? 1.f : 0.f, q + 1 >= pad ? 1.f : 0.f, q + 2 >= pad ? 1.f : 0.f,
+                        q + 3 >= pad ? 1.f : 0.f);
+  }
   WarpSmem S = carve(smem, J);
   float* store = A.store_pool + A.store_off[t];
   const uint32_t* hv = A.hvar + (size_t)t * A.WB * Kp;
@@ -264,17 +267,17 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, float4
       S.fl[(b_first & 1) * 32 + lane] = F[l];
       S.pl[(b_first & 1) * 32 + lane] = PL[l];
     }
-    fetch_words<J, W>(wl + (b_first & 1) * 32 * J, hv + (size_t)b_first * Kp, kb, G);
+    fetch_words<J, W>(wl + (b_first & 1) * 32 * J, hv + (size_t)b_first * Kp, kb);
     if (b_first != b_last) {
       const int b2 = b_first + dir;
-      fetch_words<J, W>(wl + (b2 & 1) * 32 * J, hv + (size_t)b2 * Kp, kb, G);
+      fetch_words<J, W>(wl + (b2 & 1) * 32 * J, hv + (size_t)b2 * Kp, kb);
     }
   }
   cp_commit();
   if (POST) {
 #pragma unroll
     for (int d = 0; d < kRowDepth; ++d) {
-      if (d < n) fetch_row<J, W>(rl + (d % kRing) * 32 * J, row_vec(site_of(d)), G);
+      if (d < n) fetch_row<J, W>(rl + (d % kRing) * 32 * J, row_vec(site_of(d)));
       cp_commit();
     }
   }
@@ -292,7 +295,7 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, float4
     const float4* r = row_vec(lo - 1);
 #pragma unroll
     for (int j = 0; j < J; ++j)
-      if (j < G) x[j] = r[32 * W * j];
+      x[j] = r[32 * W * j];
     acc = A.sc.asum[t];
     t_prev = T[lo - 1];
   }
@@ -300,7 +303,7 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, float4
     const float4* r = reinterpret_cast<const float4*>(A.sc.brow + (size_t)t * Ks + pb);
 #pragma unroll
     for (int j = 0; j < J; ++j)
-      if (j < G) x[j] = r[32 * W * j];
+      x[j] = r[32 * W * j];
     acc = A.sc.bsum[t];
   }
   float4 pe = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -330,7 +333,7 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, float4
         const int bn = b + dir;
         const int ln = (bn << 5) + lane;
         if (ln < np) { pe = E[ln]; pt = T[ln]; pf = F[ln]; pp = PL[ln]; }
-        fetch_words<J, W>(wl + (bn & 1) * 32 * J, hv + (size_t)bn * Kp, kb, G);
+        fetch_words<J, W>(wl + (bn & 1) * 32 * J, hv + (size_t)bn * Kp, kb);
       }
       if (!POST) {
         cp_commit();
@@ -338,7 +341,7 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, float4
       }
     }
     if (POST) {
-      if (s + kRowDepth < n) fetch_row<J, W>(rl + ((s + kRowDepth) % kRing) * 32 * J, row_vec(site_of(s + kRowDepth)), G);
+      if (s + kRowDepth < n) fetch_row<J, W>(rl + ((s + kRowDepth) % kRing) * 32 * J, row_vec(site_of(s + kRowDepth)));
       cp_commit();
       cp_wait<kRowDepth>();
     }
@@ -347,7 +350,7 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, float4
       const uint4* wb = wl + (b & 1) * 32 * J;
 #pragma unroll
       for (int j = 0; j < J; ++j)
-        if (j < G) w[j] = wb[32 * j];
+        w[j] = wb[32 * j];
     }
     const uint32_t m = 1u << i;
     const uint8_t f = S.fl[(b & 1) * 32 + i];
@@ -368,7 +371,7 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, float4
       fact2 = tt.y / acc;
     }
     const float ex = f ? 1.0f : e.x, ey = f ? 1.0f : e.y;
-    chain_step<J, W, FWD, POST, INIT>(x, w, m, q0, q1, q2, vq, G, fact1, fact2, ex, ey, rowl, srowl);
+    chain_step<J, W, FWD, POST, INIT>(x, w, m, q0, q1, q2, vf, fact1, fact2, ex, ey, rowl, srowl);
     const float v0 = warp_sum(__fadd_rn(__fadd_rn(q0[0], q0[1]), __fadd_rn(q0[2], q0[3])));
     float v1 = 0.f, v2 = 0.f;
     if (POST) {
@@ -402,7 +405,7 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, float4
       float4* r = reinterpret_cast<float4*>(A.sc.brow + (size_t)t * Ks + pb);
 #pragma unroll
       for (int j = 0; j < J; ++j)
-        if (j < G) r[32 * W * j] = x[j];
+        r[32 * W * j] = x[j];
       if (wi == 0 && lane == 0) A.sc.bsum[t] = acc;
     }
   }
@@ -433,16 +436,11 @@ size_t impute_warp_smem(int J) { return (size_t)kWarpsPerChain * kChainsPerCta *
 // Local quads per warp for at most Kmax states (the J of launch_impute_warp).
 int impute_groups(int Kmax) {
   const int W = kWarpsPerChain;
-  const int jq = ((Kmax + 127) / 128 + W - 1) / W * W;
-  const int G = jq / W;
-  return G <= 2 ? 2 : (G <= 4 ? 4 : (G + 3) / 4 * 4);
+  return std::max(1, ((Kmax + 127) / 128 + W - 1) / W);
 }
 
 // Row stride of the store in padded coordinates for at most Kmax states.
-int impute_store_stride(int Kmax) {
-  const int W = kWarpsPerChain;
-  return 128 * (((Kmax + 127) / 128 + W - 1) / W * W);
-}
+int impute_store_stride(int Kmax) { return 128 * kWarpsPerChain * impute_groups(Kmax); }
 
 template <int J, bool POST>
 static int launch_chains(const ChainArgs& a, cudaStream_t s) {
@@ -484,7 +482,8 @@ int launch_impute_warp(int phase, int J, const ModelConst& mc, ImputeWork& w, fl
 #define GP_WARP(JJ) \
   case JJ: return phase == 2 ? launch_chains<JJ, true>(a, s) : launch_chains<JJ, false>(a, s);
   switch (J) {
-    GP_WARP(2) GP_WARP(4) GP_WARP(8) GP_WARP(12) GP_WARP(16)
+    GP_WARP(1) GP_WARP(2) GP_WARP(3) GP_WARP(4) GP_WARP(5) GP_WARP(6) GP_WARP(7) GP_WARP(8)
+    GP_WARP(9) GP_WARP(10) GP_WARP(11) GP_WARP(12) GP_WARP(13) GP_WARP(14) GP_WARP(15) GP_WARP(16)
     default: return GP_E_ARG;
   }
 #undef GP_WARP
