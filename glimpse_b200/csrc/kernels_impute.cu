@@ -87,40 +87,67 @@ __global__ void k_compact_poly(const uint8_t* __restrict__ mark, int L, int32_t*
 
 // Hvar words: common sites gather the state's bit from the panel, rare sites
 // start at the major allele (conditioning_set.cpp:145-176; Hvar.set(lrel, major)).
+// One CTA per (32-site block, haplotype). The common sites of a block are
+// consecutive common rows, so they span at most two 32-bit words of a panel
+// haplotype's row (refT); the CTA first describes every site of the block by the
+// position of its bit in that 64-bit pair (or marks it rare), then each thread
+// builds the words of its states from two gathered words and register shifts.
 __global__ void k_build_hvar(const int32_t* __restrict__ poly, const int32_t* __restrict__ npoly,
                              const int32_t* __restrict__ comrow, const uint8_t* __restrict__ major,
                              const uint32_t* __restrict__ refT, int W, const uint32_t* __restrict__ states,
                              const int32_t* __restrict__ nstates, int Kp, int L, int WB,
                              uint32_t* __restrict__ hvar) {
-  const int t = blockIdx.z;
-  const int b = blockIdx.y;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ int s_row[32];
+  __shared__ uint32_t s_rmaj;
+  const int t = blockIdx.y;
+  const int b = blockIdx.x;
   const int np = npoly[t];
-  if (b * 32 >= np || k >= Kp) return;
-  uint32_t word = 0;
-  if (k < nstates[t]) {
-    const uint32_t* row = refT + (size_t)states[(size_t)t * Kp + k] * W;
-    const int32_t* pl = poly + (size_t)t * L;
-    int cached = -1;
-    uint32_t cw = 0;
-    const int n = min(32, np - b * 32);
-    for (int i = 0; i < n; ++i) {
-      const int s = pl[b * 32 + i];
-      const int r = comrow[s];
-      uint32_t bit;
-      if (r >= 0) {
-        if ((r >> 5) != cached) {
-          cached = r >> 5;
-          cw = row[cached];
-        }
-        bit = (cw >> (r & 31)) & 1u;
-      } else {
-        bit = major[s];
-      }
-      word |= bit << i;
+  if (b * 32 >= np) return;
+  const int n = min(32, np - b * 32);
+  if (threadIdx.x < 32) {
+    const int i = threadIdx.x;
+    int r = -1;
+    uint32_t maj = 0u;
+    if (i < n) {
+      const int site = poly[(size_t)t * L + b * 32 + i];
+      r = comrow[site];
+      if (r < 0) maj = major[site] ? 1u : 0u;
     }
+    s_row[i] = r;
+    const uint32_t mb = __ballot_sync(0xffffffffu, maj != 0u);
+    if (i == 0) s_rmaj = mb;
   }
-  hvar[((size_t)t * WB + b) * Kp + k] = word;
+  __syncthreads();
+  // first common row of the block (rows increase with the site)
+  int r0 = -1;
+  for (int i = 0; i < n && r0 < 0; ++i) r0 = s_row[i];
+  const uint32_t rmaj = s_rmaj;
+  const int K = nstates[t];
+  uint32_t* out = hvar + ((size_t)t * WB + b) * Kp;
+  if (r0 < 0) {  // no common site: the major alleles only
+    for (int k = threadIdx.x; k < Kp; k += blockDim.x) out[k] = k < K ? rmaj : 0u;
+    return;
+  }
+  const int w0 = r0 >> 5;
+  const bool two = w0 + 1 < W;
+  int sh[32];  // bit of site i in the (word w0, word w0 + 1) pair, or -1 for a rare site
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    const int r = i < n ? s_row[i] : -1;
+    sh[i] = r >= 0 ? r - (w0 << 5) : -1;
+  }
+  for (int k = threadIdx.x; k < Kp; k += blockDim.x) {
+    uint32_t word = 0u;
+    if (k < K) {
+      const uint32_t* row = refT + (size_t)states[(size_t)t * Kp + k] * W + w0;
+      const uint64_t pair = (uint64_t)row[0] | (two ? (uint64_t)row[1] << 32 : 0ull);
+      word = rmaj;
+#pragma unroll
+      for (int i = 0; i < 32; ++i)
+        if (sh[i] >= 0) word |= (uint32_t)((pair >> sh[i]) & 1ull) << i;
+    }
+    out[k] = word;
+  }
 }
 
 // Rare carriers among the states flip their bit to the non-major allele
@@ -240,7 +267,7 @@ void launch_compact_poly(const DevPanel& P, ImputeWork& w, cudaStream_t s) {
 }
 
 void launch_build_hvar(const DevPanel& P, ImputeWork& w, cudaStream_t s) {
-  dim3 g((w.Kp + 127) / 128, w.WB, w.n);
+  dim3 g(w.WB, w.n);
   k_build_hvar<<<g, 128, 0, s>>>(w.poly.as<int32_t>(), w.npoly.as<int32_t>(), P.comrow, P.major, P.refT, P.W,
                                  w.states.as<uint32_t>(), w.nstates.as<int32_t>(), w.Kp, P.L, w.WB,
                                  w.hvar.as<uint32_t>());

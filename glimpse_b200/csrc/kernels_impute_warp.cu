@@ -8,7 +8,8 @@
 // largest K of the call) and warp w, lane `lane`, local quad j owns the 4
 // consecutive padded states 128 (W j + w) + 4 lane + c, c = 0..3 (state k =
 // padded index - pad). Every chain runs all J quads, so a site is one
-// straight-line block for the scheduler; padded states are held at 0. Rows of
+// straight-line block for the scheduler; padded states are held at 0, and quads
+// without a state are neither stored nor fetched. Rows of
 // the store are kept in padded coordinates with stride Ks, so a lane's 4 values
 // of a row are one aligned 16-byte vector: phase 1 writes a row with one 16-byte
 // store per lane and quad, phase 2 stages rows with 16-byte cp.async. The
@@ -146,7 +147,8 @@ __device__ __forceinline__ float compf(const float4& v, int c) { return c == 0 ?
 // padded states (vf = 0) are kept at 0, and the vectors are written whole.
 template <int J, int W, bool FWD, bool POST, bool INIT>
 __device__ __forceinline__ void chain_step(float4 (&x)[J], const uint4 (&w)[J], uint32_t m, float (&q0)[4],
-                                           float (&q1)[4], float (&q2)[4], const float4 (&vf)[J], float fact1,
+                                           float (&q1)[4], float (&q2)[4], const float4 (&vf)[J], uint32_t qmask,
+                                           float fact1,
                                            float fact2, float ex, float ey, const float4* rowl, float4* srowl) {
 #pragma unroll
   for (int j = 0; j < J; ++j) {
@@ -172,7 +174,7 @@ __device__ __forceinline__ void chain_step(float4 (&x)[J], const uint4 (&w)[J], 
         comp(st, c) = FWD ? nx : (INIT ? 1.0f : pcv);
       }
     }
-    if (!POST) srowl[32 * W * j] = st;
+    if (!POST && ((qmask >> j) & 1u)) srowl[32 * W * j] = st;
   }
 }
 
@@ -212,11 +214,10 @@ __device__ __forceinline__ void fetch_words(uint4* dst, const uint32_t* row, int
 // This lane's vectors of a stored row (padded coordinates; quad j at vector
 // offset 32 W j from the lane's quad 0) into dst[32 j].
 template <int J, int W>
-__device__ __forceinline__ void fetch_row(float4* dst, const float4* rowl) {
+__device__ __forceinline__ void fetch_row(float4* dst, const float4* rowl, uint32_t qmask) {
 #pragma unroll
-  for (int j = 0; j < J; ++j) {
-    cp_async16(dst + 32 * j, rowl + 32 * W * j);
-  }
+  for (int j = 0; j < J; ++j)
+    if ((qmask >> j) & 1u) cp_async16(dst + 32 * j, rowl + 32 * W * j);
 }
 
 template <int J, int W, bool FWD, bool POST>
@@ -234,11 +235,13 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, float4
   const int pb = 128 * wi + 4 * lane;  // padded index of this lane's quad 0
   const int kb = pb - pad;             // its state index
   float4 vf[J];                        // 1 for a state, 0 for padding
+  uint32_t qmask = 0u;                 // bit j: quad j holds at least one state (is stored and fetched)
 #pragma unroll
   for (int j = 0; j < J; ++j) {
     const int q = pb + 128 * W * j;
     vf[j] = make_float4(q >= pad ? 1.f : 0.f, q + 1 >= pad ? 1.f : 0.f, q + 2 >= pad ? 1.f : 0.f,
                         q + 3 >= pad ? 1.f : 0.f);
+    if (q + 3 >= pad) qmask |= 1u << j;
   }
   WarpSmem S = carve(smem, J);
   float* store = A.store_pool + A.store_off[t];
@@ -255,6 +258,15 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, float4
   constexpr int dir = FWD ? 1 : -1;
   uint4* wl = S.words + lane;   // this lane's words; block buffer (b & 1) at offset 32 J (b & 1)
   float4* rl = S.ring + lane;   // this lane's staged row vectors; slot s at offset 32 J s
+
+  // Ring entries of fully padded quads are never fetched; they hold 0.
+  if (POST) {
+#pragma unroll
+    for (int d = 0; d < kRing; ++d)
+#pragma unroll
+      for (int j = 0; j < J; ++j)
+        if (!((qmask >> j) & 1u)) rl[(d * J + j) * 32] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
 
   // ---- prologue: records and Hvar words of the first two blocks, first rows ----
   const int b_first = site_of(0) >> 5;
@@ -277,7 +289,7 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, float4
   if (POST) {
 #pragma unroll
     for (int d = 0; d < kRowDepth; ++d) {
-      if (d < n) fetch_row<J, W>(rl + (d % kRing) * 32 * J, row_vec(site_of(d)));
+      if (d < n) fetch_row<J, W>(rl + (d % kRing) * 32 * J, row_vec(site_of(d)), qmask);
       cp_commit();
     }
   }
@@ -295,7 +307,7 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, float4
     const float4* r = row_vec(lo - 1);
 #pragma unroll
     for (int j = 0; j < J; ++j)
-      x[j] = r[32 * W * j];
+      if ((qmask >> j) & 1u) x[j] = r[32 * W * j];
     acc = A.sc.asum[t];
     t_prev = T[lo - 1];
   }
@@ -341,7 +353,8 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, float4
       }
     }
     if (POST) {
-      if (s + kRowDepth < n) fetch_row<J, W>(rl + ((s + kRowDepth) % kRing) * 32 * J, row_vec(site_of(s + kRowDepth)));
+      if (s + kRowDepth < n)
+        fetch_row<J, W>(rl + ((s + kRowDepth) % kRing) * 32 * J, row_vec(site_of(s + kRowDepth)), qmask);
       cp_commit();
       cp_wait<kRowDepth>();
     }
@@ -371,7 +384,7 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, float4
       fact2 = tt.y / acc;
     }
     const float ex = f ? 1.0f : e.x, ey = f ? 1.0f : e.y;
-    chain_step<J, W, FWD, POST, INIT>(x, w, m, q0, q1, q2, vf, fact1, fact2, ex, ey, rowl, srowl);
+    chain_step<J, W, FWD, POST, INIT>(x, w, m, q0, q1, q2, vf, qmask, fact1, fact2, ex, ey, rowl, srowl);
     const float v0 = warp_sum(__fadd_rn(__fadd_rn(q0[0], q0[1]), __fadd_rn(q0[2], q0[3])));
     float v1 = 0.f, v2 = 0.f;
     if (POST) {
