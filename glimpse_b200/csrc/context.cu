@@ -305,6 +305,12 @@ int Context::run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
     return cuda_fail(e, "alloc split");
   cudaMemcpyAsync(w.alpha_off.ptr, aoff.data(), n * 8, cudaMemcpyHostToDevice, stream);
   cudaMemcpyAsync(w.split.ptr, split.data(), n * 4, cudaMemcpyHostToDevice, stream);
+  // Chains of the longest haplotypes (most poly sites) are launched first.
+  std::vector<int32_t> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return impute_np[x] > impute_np[y]; });
+  if ((e = w.order.ensure((size_t)n * 4)) != cudaSuccess) return cuda_fail(e, "alloc order");
+  cudaMemcpyAsync(w.order.ptr, order.data(), (size_t)n * 4, cudaMemcpyHostToDevice, stream);
   launch_site_records(panel, mc, w, d_hl, d_flat, stream);
   double cells = 0;
   for (int i = 0; i < n; ++i) cells += (double)impute_np[i] * (double)host_nstates[i];
@@ -395,6 +401,19 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   S.of1 = p.of1.as<float>();
   S.dip = p.dip.as<int32_t>();
   S.err = p.err.as<int32_t>();
+  // Blocks in decreasing order of work (VAR sites x state groups), so that the
+  // heaviest targets start first and share an SM with the lightest.
+  std::vector<int32_t> order(nb);
+  std::vector<double> cost(nb);
+  for (int b = 0; b < nb; ++b) {
+    const int t = tsel_host.empty() ? b : tsel_host[b];
+    order[b] = b;
+    cost[b] = (double)cnt[b] * (1.0 + (double)((host_nstates[t] + kPhaseThreads - 1) / kPhaseThreads));
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+  if ((e = p.order.ensure((size_t)nb * 4)) != cudaSuccess) return cuda_fail(e, "alloc order");
+  cudaMemcpyAsync(p.order.ptr, order.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, stream);
+  S.order = p.order.as<int32_t>();
   const int J = std::max(1, (Kmax + kPhaseThreads - 1) / kPhaseThreads);
   double pcells = 0;
   for (int b = 0; b < nb; ++b) {

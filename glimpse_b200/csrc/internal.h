@@ -70,16 +70,17 @@ struct ImputeWork {
   DevBuf mark, polyidx, poly, npoly;
   DevBuf hvar, em, tr, fl;
   DevBuf alpha, alpha_off, split, split_scr;
+  DevBuf order;  // [n] haplotypes in decreasing order of poly sites (chain launch order); ptr null: identity
   DevBuf hl, hp, flat;
 };
 
 // Scratch of the phasing HMM.
 struct PhaseWork {
   DevBuf rel, code, seg, miss, seg_start, counts, ytp, ytn, vflags, recb, recf;
-  DevBuf pprob, iprob, offs, pprob_sum, pprob_sumsum, iprob_sum, of1, dip, err;
+  DevBuf pprob, iprob, offs, pprob_sum, pprob_sumsum, iprob_sum, of1, dip, err, order;
   std::vector<DevBuf*> all() {
     return {&rel, &code, &seg, &miss, &seg_start, &counts, &ytp, &ytn, &vflags, &recb, &recf, &pprob, &iprob, &offs,
-            &pprob_sum, &pprob_sumsum, &iprob_sum, &of1, &dip, &err};
+            &pprob_sum, &pprob_sumsum, &iprob_sum, &of1, &dip, &err, &order};
   }
 };
 

@@ -194,6 +194,7 @@ struct ChainArgs {
   int L, WB, Kp, Ks;
   ModelConst mc;
   float* __restrict__ hp;
+  const int32_t* __restrict__ order;  // [n] haplotype of chain pair c (longest first), or null for the identity
 };
 
 // Hvar words of this lane's states (state index kb + 128 W j + c) of one block
@@ -425,8 +426,8 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, float4
 }
 
 // Chain c = blockIdx.x * kChainsPerCta + (warp / W) is run by the W warps
-// (warp % W = 0..W-1) of its slot: target c / 2, forward for even chains and
-// backward for odd ones. Every warp of a chain takes the same branches, so the
+// (warp % W = 0..W-1) of its slot: haplotype order[c / 2] (c / 2 without an
+// order), forward for even chains and backward for odd ones. Every warp of a chain takes the same branches, so the
 // chain's named barrier (id 1 + slot) always sees all 32 W threads.
 template <int J, int W, bool POST>
 __global__ void __launch_bounds__(32 * W * kChainsPerCta) k_impute_warp(ChainArgs A) {
@@ -438,8 +439,9 @@ __global__ void __launch_bounds__(32 * W * kChainsPerCta) k_impute_warp(ChainArg
   const int chain = blockIdx.x * kChainsPerCta + slot;
   if (chain >= A.nchains) return;
   char* smem = smem_raw + (size_t)warp * warp_smem_bytes(J);
-  if ((chain & 1) == 0) run_chain<J, W, true, POST>(A, smem, xch[slot], chain >> 1, wi, lane, 1 + slot);
-  else run_chain<J, W, false, POST>(A, smem, xch[slot], chain >> 1, wi, lane, 1 + slot);
+  const int t = A.order ? A.order[chain >> 1] : chain >> 1;
+  if ((chain & 1) == 0) run_chain<J, W, true, POST>(A, smem, xch[slot], t, wi, lane, 1 + slot);
+  else run_chain<J, W, false, POST>(A, smem, xch[slot], t, wi, lane, 1 + slot);
 }
 
 }  // namespace
@@ -492,6 +494,7 @@ int launch_impute_warp(int phase, int J, const ModelConst& mc, ImputeWork& w, fl
   a.Ks = w.Ks;
   a.mc = mc;
   a.hp = hp;
+  a.order = w.order.as<int32_t>();
 #define GP_WARP(JJ) \
   case JJ: return phase == 2 ? launch_chains<JJ, true>(a, s) : launch_chains<JJ, false>(a, s);
   switch (J) {

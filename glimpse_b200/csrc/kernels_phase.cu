@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(PT, 2) k_phase(const int32_t* __restrict__ tse
   __shared__ PhaseShared sm;
   __shared__ VarStage vs;
   int buf = 0;
-  const int b = blockIdx.x;
+  const int b = S.order ? S.order[blockIdx.x] : blockIdx.x;
   const int t = tsel ? tsel[b] : b;
   const int K = nstates[t];
   const int nv = V.nvar[b];

@@ -41,6 +41,7 @@ struct PhaseStore {
   float* of1;            // imputeProbOf1s [b][L][8]
   int32_t* dip;          // dip_sampled [b][L+2]
   int32_t* err;          // [b] nonzero when a diplotype draw saw an invalid sum
+  const int32_t* order;  // [nb] batch entry of each block of k_phase (heaviest first), or null for the identity
 };
 
 void launch_build_vars(const int32_t* tsel, int nb, const int32_t* poly, const int32_t* npoly, const uint8_t* h0,
