@@ -145,37 +145,80 @@ __device__ __forceinline__ float compf(const float4& v, int c) { return c == 0 ?
 // its stored row vector (global, quad j at offset 32 W j). Every chain of a
 // launch runs the launch's J quads, so a site is one straight-line block; the
 // padded states (vf = 0) are kept at 0, and the vectors are written whole.
+// Two floats in one 64-bit register pair (lo = first); the packed mul / add /
+// fma round each element exactly as the scalar instructions do.
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 f2_pack(float lo, float hi) {
+  f2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(f2 v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2 f2_fma(f2 a, f2 b, f2 c) {
+  f2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ f2 f2_mul(f2 a, f2 b) {
+  f2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2 f2_add(f2 a, f2 b) {
+  f2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+
 template <int J, int W, bool FWD, bool POST, bool INIT>
 __device__ __forceinline__ void chain_step(float4 (&x)[J], const uint4 (&w)[J], uint32_t m, float (&q0)[4],
                                            float (&q1)[4], float (&q2)[4], const float4 (&vf)[J], uint32_t qmask,
                                            float fact1,
                                            float fact2, float ex, float ey, const float4* rowl, float4* srowl) {
+  // components (0, 1) and (2, 3) of a quad are processed as packed pairs
+  const f2 fact1p = f2_pack(fact1, fact1), fact2p = f2_pack(fact2, fact2);
+  f2 q0p[2] = {f2_pack(q0[0], q0[1]), f2_pack(q0[2], q0[3])};
 #pragma unroll
   for (int j = 0; j < J; ++j) {
     float4 r4 = make_float4(0.f, 0.f, 0.f, 0.f);
     if (POST) r4 = rowl[32 * j];
     float4 st;
+    bool bit[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) bit[c] = (compu(w[j], c) & m) != 0u;
+    const f2 xp[2] = {f2_pack(x[j].x, x[j].y), f2_pack(x[j].z, x[j].w)};
+    const f2 vp[2] = {f2_pack(vf[j].x, vf[j].y), f2_pack(vf[j].z, vf[j].w)};
+    float pcv[4], nx[4];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const f2 pc = INIT ? fact1p : f2_fma(xp[h], fact2p, fact1p);
+      const f2 e = f2_pack(bit[2 * h] ? ey : ex, bit[2 * h + 1] ? ey : ex);
+      // padded states are multiplied by 0, valid ones by 1 (exact)
+      const f2 n2 = f2_mul(f2_mul(pc, e), vp[h]);
+      q0p[h] = f2_add(q0p[h], n2);
+      f2_unpack(pc, pcv[2 * h], pcv[2 * h + 1]);
+      f2_unpack(n2, nx[2 * h], nx[2 * h + 1]);
+    }
+    x[j] = make_float4(nx[0], nx[1], nx[2], nx[3]);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      const bool bit = (compu(w[j], c) & m) != 0u;
-      const float pcv = INIT ? fact1 : fmaf(compf(x[j], c), fact2, fact1);
-      // padded states are multiplied by 0, valid ones by 1 (exact)
-      const float nx = __fmul_rn(__fmul_rn(pcv, bit ? ey : ex), compf(vf[j], c));
-      comp(x[j], c) = nx;
-      q0[c] = __fadd_rn(q0[c], nx);
       if (POST) {
         const float r = compf(r4, c);
         float d;
-        if (FWD) d = __fmul_rn(nx, r);           // alpha x stored prob_curr (1 at the last site)
-        else d = INIT ? r : __fmul_rn(r, pcv);  // stored alpha x prob_curr; alpha alone at the last site
-        if (bit) q2[c] = __fadd_rn(q2[c], d);
+        if (FWD) d = __fmul_rn(nx[c], r);           // alpha x stored prob_curr (1 at the last site)
+        else d = INIT ? r : __fmul_rn(r, pcv[c]);  // stored alpha x prob_curr; alpha alone at the last site
+        if (bit[c]) q2[c] = __fadd_rn(q2[c], d);
         else q1[c] = __fadd_rn(q1[c], d);
       } else {
-        comp(st, c) = FWD ? nx : (INIT ? 1.0f : pcv);
+        comp(st, c) = FWD ? nx[c] : (INIT ? 1.0f : pcv[c]);
       }
     }
     if (!POST && ((qmask >> j) & 1u)) srowl[32 * W * j] = st;
   }
+  f2_unpack(q0p[0], q0[0], q0[1]);
+  f2_unpack(q0p[1], q0[2], q0[3]);
 }
 
 // Arguments of one launch, shared by the forward and backward chains.
