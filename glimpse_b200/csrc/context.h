@@ -34,13 +34,13 @@ struct TargetWork {
   DevBuf gp0, gp1, gpflags, ds, gt0, gt1;
   DevBuf sind, nsind, bitmap;
   DevBuf d_hap_target, d_hap_which, d_target_hap0, d_target_nhap, d_kpbwt, tar_hap, d_grp;
-  DevBuf push_key, push_id, push_cnt, stored_bits, start_idx, overflow, carry;
+  DevBuf push_key, push_id, push_cnt, stored_bits, start_idx, overflow, carry, ebits;
   int stored_cnt = 0;
   bool finalized = false;
   std::vector<DevBuf*> all() {
     return {&gl, &flat, &ploidy, &dip_list, &h0, &h1, &hl, &hp0, &hp1, &gp0, &gp1, &gpflags, &ds, &gt0, &gt1,
             &sind, &nsind, &bitmap, &d_hap_target, &d_hap_which, &d_target_hap0, &d_target_nhap, &d_kpbwt,
-            &tar_hap, &d_grp, &push_key, &push_id, &push_cnt, &stored_bits, &start_idx, &overflow, &carry};
+            &tar_hap, &d_grp, &push_key, &push_id, &push_cnt, &stored_bits, &start_idx, &overflow, &carry, &ebits};
   }
 };
 

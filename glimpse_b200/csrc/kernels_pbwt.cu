@@ -168,6 +168,35 @@ __device__ __forceinline__ bool any_carrier(const uint32_t* __restrict__ c, int 
   return false;
 }
 
+// The per-haplotype bit of every sweep event (PbwtSelectArgs::ebits): the
+// allele H[k] at an HQ common site k, or for a run of rare sites [k0, kend] the
+// init_rare test (haplotype_set.cpp:655-680), sn > 0 and a carrier bit in the run.
+// The sweep reads one word per 32 events, a chunk ahead, instead of a scattered
+// byte or carrier load per event on its sequential path. Thread x of a block is
+// haplotype blockIdx.x * blockDim.x + x, and blockIdx.y the chunk of 32 events,
+// so the event records a warp reads are the same for all its lanes.
+__global__ void k_event_bits(PbwtSelectArgs a) {
+  const int hp = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  if (hp >= a.n_haps) return;
+  const int nev = a.P.n_events;
+  const int t = a.hap_target[hp];
+  const uint8_t* H = (a.hap_which[hp] ? a.h1 : a.h0) + (size_t)t * a.L;
+  const uint32_t* carry = a.carry + (size_t)hp * a.Wc;
+  uint32_t bits = 0u;
+  const int n = min(32, nev - (c << 5));
+  for (int i = 0; i < n; ++i) {
+    const int e = (c << 5) + i;
+    const int4 r0 = a.P.events[2 * e];
+    const int4 r1 = a.P.events[2 * e + 1];
+    bool b;
+    if (!(r0.x & (1 << 30))) b = H[r0.x] != 0;
+    else b = r1.x > 0 && any_carrier(carry, r0.x & ~(1 << 30), r0.z);
+    if (b) bits |= 1u << i;
+  }
+  a.ebits[(size_t)hp * a.We + c] = bits;
+}
+
 // One warp per block; lane = one target haplotype. The lanes of a warp walk the
 // event list (non-LQ common sites and runs of rare sites) in step: every branch
 // that skips work is warp-uniform. Shared memory per warp holds
@@ -218,7 +247,10 @@ __global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D) {
   const int L = a.L;
   const int t = a.hap_target[hp];
   const uint8_t* H = (a.hap_which[hp] ? a.h1 : a.h0) + (size_t)t * L;
-  const uint32_t* carry = a.carry + (size_t)hp * a.Wc;
+  // event bits of the current chunk and of the next one
+  const uint32_t* eb = a.ebits + (size_t)hp * a.We;
+  uint32_t ebw = a.We > 0 ? eb[0] : 0u;
+  uint32_t ebn = a.We > 1 ? eb[1] : 0u;
   Pusher pu{a.push_key + (size_t)hp * K * a.cap, a.push_id + (size_t)hp * K * a.cap, scnt, a.cap, a.overflow};
   for (int o = 0; o < K; ++o) scnt[o * 32] = 0;
   int idx = a.start_idx[hp], f = 0, g = N;
@@ -235,7 +267,10 @@ __global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D) {
     if ((e & 31) == 0 && e > 0) {
       __syncwarp(live);  // chunk c - 1 is no longer read
       load_chunk(c + 1);
+      ebw = ebn;
+      ebn = c + 1 < a.We ? eb[c + 1] : 0u;
     }
+    const bool ebit = (ebw >> (e & 31)) & 1u;
     const int4 r0 = evbuf[((c & 1) * 32 + (e & 31)) * 2];
     const int4 r1 = evbuf[((c & 1) * 32 + (e & 31)) * 2 + 1];
     const int sn = r1.x;
@@ -286,7 +321,7 @@ __global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D) {
       }
       // select_common_pd_fg at HQ common site l
       const int prev_hap = tar;
-      const int al = H[k];
+      const int al = ebit ? 1 : 0;  // H[k]
       tar = al;
       const int vi = rank_v(row, row + Wv, idx), vf = rank_v(row, row + Wv, f), vg = rank_v(row, row + Wv, g);
       if (D > 0) {
@@ -326,7 +361,7 @@ __global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D) {
       // ---------------- run of rare sites [k0, kend] ----------------
       const int k0 = r0.x & ~(1 << 30), kend = r0.z, so = r0.w;
       // init_rare: is this haplotype in rareTarHaps for the run?
-      in_rare = sn > 0 && any_carrier(carry, k0, kend);
+      in_rare = ebit;  // sn > 0 and a carrier bit in [k0, kend]
       // Nothing happens at the run's sites for a haplotype outside rareTarHaps;
       // when no haplotype of the warp is in it, the warp goes on to the next event.
       if (__all_sync(live, !in_rare)) continue;
@@ -437,6 +472,7 @@ __global__ void k_pbwt_union(PbwtSelectArgs a) {
 void launch_pbwt_select(const PbwtSelectArgs& a, cudaStream_t s) {
   k_pbwt_rng<<<1, 32, 0, s>>>(a);
   k_rare_carriers<<<dim3((a.Wc + 127) / 128, a.n_haps), 128, 0, s>>>(a);
+  if (a.We > 0) k_event_bits<<<dim3((a.n_haps + 127) / 128, a.We), 128, 0, s>>>(a);
   // Ring of D rank rows, D <= 8, within 96 KB.
   const size_t slot_bytes = (size_t)a.P.R * 4;
   int D = (int)std::min<size_t>(8, (96u << 10) / slot_bytes);

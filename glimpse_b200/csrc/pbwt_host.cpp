@@ -513,6 +513,12 @@ int Context::pbwt_select_states(int stage, int iteration, int Kp) {
     if (ec != cudaSuccess) return cuda_fail(ec, "alloc carry");
   }
   a.carry = T.carry.as<uint32_t>();
+  a.We = (pbwt.n_events + 31) / 32;
+  {
+    cudaError_t ec = T.ebits.ensure((size_t)a.n_haps * std::max(a.We, 1) * 4);
+    if (ec != cudaSuccess) return cuda_fail(ec, "alloc event bits");
+  }
+  a.ebits = T.ebits.as<uint32_t>();
   a.start_idx = T.start_idx.as<int32_t>();
   a.tar_hap = T.tar_hap.as<uint8_t>();
   a.push_key = T.push_key.as<uint32_t>();
@@ -528,7 +534,7 @@ int Context::pbwt_select_states(int stage, int iteration, int Kp) {
   a.iteration = iteration;
   cudaMemsetAsync(T.overflow.ptr, 0, 4, stream);
   launch_pbwt_select(a, stream);
-  prof.kernel_launches += 4;
+  prof.kernel_launches += 5;
   int32_t ovf = 0;
   cudaMemcpyAsync(&ovf, T.overflow.ptr, 4, cudaMemcpyDeviceToHost, stream);
   cudaError_t e = cudaStreamSynchronize(stream);

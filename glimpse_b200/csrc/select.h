@@ -83,6 +83,10 @@ struct PbwtSelectArgs {
   uint32_t* stored_bits;      // [ceil(n_com_hq/32)]
   uint32_t* carry;            // [n_haps][Wc]: bit k = non-LQ rare site k where the haplotype has the non-major allele
   int Wc;                     // ceil(L / 32)
+  uint32_t* ebits;            // [n_haps][We]: bit (e & 31) of word e >> 5 is, for event e of the sweep, the
+                              // haplotype's allele at that HQ common site, or for a run of rare sites, whether it
+                              // carries a non-major allele at a non-LQ site of the run
+  int We;                     // ceil(n_events / 32)
   int32_t* start_idx;         // [n_haps] random pbwt_index
   uint8_t* tar_hap;           // [n_haps] persistent across iterations
   uint32_t* push_key;         // [n_haps][depth][cap]
