@@ -4,6 +4,8 @@
   * burn-in/main: matchHapsFromCompressedPBWTSmall (haplotype_set.cpp:317-394),
     every pbwt_states level list, and the conditioning_set::compactSelection
     union (conditioning_set.cpp:96-104)."""
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -59,3 +61,38 @@ def test_pbwt_selection_matches_reference(pair, it, noise):
             assert np.array_equal(r, g), f"target {t} level {lv}: {r[:10]} vs {g[:10]} ({len(r)} vs {len(g)})"
         ref_states = orc.select(t, O.STAGE_BURN)
         assert np.array_equal(ref_states, ctx.states(t)), f"target {t} union differs"
+
+
+@pytest.fixture(scope="module")
+def pair_haploid(small_workload):
+    """The small workload with target 1 haploid: 5 target haplotypes, an odd count,
+    so the last warp of the PBWT sweep runs a partial group."""
+    O = ref_oracle_or_skip()
+    from glimpse_b200 import native
+    w = small_workload
+    T = dataclasses.replace(w.targets, ploidy=w.targets.ploidy.copy())
+    T.ploidy[1] = 1
+    kw = dict(kinit=200, kpbwt=int(T.kpbwt.max()), pbwt_depth=8, pbwt_modulo_cm=0.05)
+    orc = O.RefOracle(w.panel, T, kpbwt_target=T.kpbwt, **kw)
+    ctx = native.Context(w.panel, **kw)
+    ctx.set_targets(T, kpbwt=T.kpbwt)
+    return w, T, orc, ctx, O
+
+
+@pytest.mark.gpu
+def test_pbwt_selection_haploid_target_matches_reference(pair_haploid):
+    w, T, orc, ctx, O = pair_haploid
+    rng = np.random.default_rng(11)
+    h0 = np.stack([_noisy(rng, T.truth[t, 0], 0.02) for t in range(T.n)])
+    h1 = np.stack([_noisy(rng, T.truth[t, 1], 0.02) for t in range(T.n)])
+    for t in range(T.n):
+        orc.set_haps(t, h0[t], h1[t])
+    ctx.set_haps(h0, h1)
+    orc.pbwt_select(4, main_iteration=False)
+    ctx.select(O.STAGE_BURN, 4)
+    for t in range(T.n):
+        ref_lv = orc.pbwt_states(t)
+        got_lv = ctx.pbwt_states(t, depth=len(ref_lv))
+        for lv, (r, g) in enumerate(zip(ref_lv, got_lv)):
+            assert np.array_equal(r, g), f"target {t} level {lv}: {len(r)} vs {len(g)}"
+        assert np.array_equal(orc.select(t, O.STAGE_BURN), ctx.states(t)), f"target {t} union differs"
