@@ -226,6 +226,8 @@ Context::~Context() {
   for (DevBuf* b : phase.all()) b->release();
   for (DevBuf* b : tw.all()) b->release();
   scratch_h0.release(); scratch_h1.release(); scratch_ids.release();
+  glin_src.release(); glin_nval.release(); glin_ploidy.release(); glin_gl.release(); glin_flat.release();
+  glin_err.release();
   if (stream) cudaStreamDestroy(stream);
 }
 

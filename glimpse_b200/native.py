@@ -23,7 +23,7 @@ EXPORTS = [
     "gp_impute_batch", "gp_rephase_batch", "gp_select", "gp_pbwt_states_get", "gp_sparse_pbwt_get",
     "gp_stage_times", "gp_build_sparse_pbwt", "gp_profile_get", "gp_profile_reset", "gp_stream",
     "gp_impute_one_static",
-    "gp_targets_reset",
+    "gp_targets_reset", "gp_gl_from_pl", "gp_gl_from_float",
 ]
 
 
@@ -183,6 +183,23 @@ class Context:
         self._check(self.lib.gp_impute_one_static(self.h, st.size, _p(st, C.c_uint32), _p(hl, C.c_float),
                                                   _p(flat, C.c_uint8), _p(hp, C.c_float)))
         return hp
+
+    def gl_from_format(self, fmt, src, ploidy, site_nval=None):
+        """gp_gl_from_pl (fmt "PL", int32 values) or gp_gl_from_float (fmt "GL",
+        float values): src[l, i, c] for site l, target i, value c < max(ploidy) + 1.
+        Returns gl (n, L, 3) uint8 and flat (n, L) uint8."""
+        ploidy = np.ascontiguousarray(ploidy, np.int32)
+        n = ploidy.size
+        L = src.shape[0]
+        dt, ct, fn = ((np.int32, C.c_int32, self.lib.gp_gl_from_pl) if fmt == "PL"
+                      else (np.float32, C.c_float, self.lib.gp_gl_from_float))
+        src = np.ascontiguousarray(src, dt)
+        nval = None if site_nval is None else np.ascontiguousarray(site_nval, np.int32)
+        gl = np.zeros((n, L, 3), np.uint8)
+        flat = np.zeros((n, L), np.uint8)
+        self._check(fn(self.h, n, L, _p(src, ct), _p(nval, C.c_int32), _p(ploidy, C.c_int32), _p(gl, C.c_uint8),
+                       _p(flat, C.c_uint8)))
+        return gl, flat
 
     def rephase_batch(self, states_list, h0, h1, flat, iteration, target_ids=None):
         """phasing_hmm::rephaseHaplotypes for len(states_list) diploid targets."""

@@ -91,6 +91,22 @@ const char* gp_last_error(const gp_ctx* ctx);
 int gp_targets_set(gp_ctx* ctx, int32_t n, const uint8_t* gl, const uint8_t* flat, const int32_t* ploidy,
                    const int32_t* kpbwt);
 
+/* Target GL input (genotype_reader::readTargetGenotypes, genotype_reader.cpp:427-500):
+ * the FORMAT/PL (int32) or FORMAT/GL (float) values of n targets at L sites,
+ * as htslib's bcf_get_format_int32 / bcf_get_format_float return them per
+ * site, packed site after site: value c of target i at site l is
+ * src[(l * n + i) * P + c], P = max(ploidy) + 1. site_nval[l] is the value
+ * count htslib returned for site l (NULL: n * P at every site); a site whose
+ * count / n differs from P is skipped, as the reference skips it. Writes gl
+ * (n x L x 3 phred bytes: PL, or lroundf(-10 GL), clamped to 255) and flat
+ * (n x L), the layout gp_targets_set takes. Absent values (missing or vector
+ * end) leave a target's site at phred 0 and flat. A negative PL or a positive
+ * GL returns GP_E_DATA naming the first such (site, target). */
+int gp_gl_from_pl(gp_ctx* ctx, int32_t n, int32_t L, const int32_t* pl, const int32_t* site_nval,
+                  const int32_t* ploidy, uint8_t* gl, uint8_t* flat);
+int gp_gl_from_float(gp_ctx* ctx, int32_t n, int32_t L, const float* glf, const int32_t* site_nval,
+                     const int32_t* ploidy, uint8_t* gl, uint8_t* flat);
+
 /* One Gibbs iteration over all targets (caller::phase_iteration,
  * caller_algorithm.cpp:86-126, with phase_individual :53-84 for every target):
  * selection, haplotype likelihoods, two imputation passes with sampling,
