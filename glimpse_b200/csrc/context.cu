@@ -228,6 +228,7 @@ Context::~Context() {
   scratch_h0.release(); scratch_h1.release(); scratch_ids.release();
   glin_src.release(); glin_nval.release(); glin_ploidy.release(); glin_gl.release(); glin_flat.release();
   glin_err.release();
+  out_gp.release(); out_site.release();
   if (stream) cudaStreamDestroy(stream);
 }
 

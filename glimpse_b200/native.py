@@ -23,7 +23,7 @@ EXPORTS = [
     "gp_impute_batch", "gp_rephase_batch", "gp_select", "gp_pbwt_states_get", "gp_sparse_pbwt_get",
     "gp_stage_times", "gp_build_sparse_pbwt", "gp_profile_get", "gp_profile_reset", "gp_stream",
     "gp_impute_one_static",
-    "gp_targets_reset", "gp_gl_from_pl", "gp_gl_from_float",
+    "gp_targets_reset", "gp_gl_from_pl", "gp_gl_from_float", "gp_output_records",
 ]
 
 
@@ -183,6 +183,16 @@ class Context:
         self._check(self.lib.gp_impute_one_static(self.h, st.size, _p(st, C.c_uint32), _p(hl, C.c_float),
                                                   _p(flat, C.c_uint8), _p(hp, C.c_float)))
         return hp
+
+    def output_records(self):
+        """gp_output_records after finalize: gp (n, L, 3) float32 as written, and per
+        site raf, af, info (L,) float32."""
+        n, L = self.n_targets, self.L
+        gp = np.zeros((n, L, 3), np.float32)
+        raf, af, info = (np.zeros(L, np.float32) for _ in range(3))
+        self._check(self.lib.gp_output_records(self.h, _p(gp, C.c_float), _p(raf, C.c_float), _p(af, C.c_float),
+                                               _p(info, C.c_float)))
+        return gp, raf, af, info
 
     def gl_from_format(self, fmt, src, ploidy, site_nval=None):
         """gp_gl_from_pl (fmt "PL", int32 values) or gp_gl_from_float (fmt "GL",

@@ -139,6 +139,15 @@ int gp_states_get(gp_ctx* ctx, int32_t target, uint32_t* states, int32_t* n_out)
 int gp_finalize(gp_ctx* ctx);
 int gp_gp_get(gp_ctx* ctx, float* gp0, float* gp1, float* ds, uint8_t* gt0, uint8_t* gt1);
 
+/* The record fields genotype_writer::writeGenotypes computes beyond GT and DS
+ * (genotype_writer.cpp:110-190), after gp_finalize: gp (n x L x 3) the FORMAT/GP
+ * values as written (floored to 1e-3, then raised by 1e-3 in the writer's order
+ * until they sum to 0.9999; a haploid target's third value is htslib's
+ * vector-end marker), and per site raf (calt / (calt + cref)), af (sum of DS over
+ * target haplotypes) and info (the INFO score; 1 unless every target is
+ * diploid and 0 < af < 1; the writer omits it for mixed ploidy). */
+int gp_output_records(gp_ctx* ctx, float* gp, float* raf, float* af, float* info);
+
 /* ---- Call-level entry points (one reference method, batched) ---- */
 
 /* imputation_hmm::computePosteriors(HL, flat, HP) (imputation_hmm.h:59)
