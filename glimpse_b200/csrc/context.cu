@@ -229,6 +229,7 @@ Context::~Context() {
   glin_src.release(); glin_nval.release(); glin_ploidy.release(); glin_gl.release(); glin_flat.release();
   glin_err.release();
   out_gp.release(); out_site.release();
+  lig_a.release(); lig_b.release(); lig_s.release(); lig_cnt.release();
   if (stream) cudaStreamDestroy(stream);
 }
 

@@ -60,6 +60,7 @@ struct Context {
   DevBuf scratch_h0, scratch_h1, scratch_ids;
   DevBuf glin_src, glin_nval, glin_ploidy, glin_gl, glin_flat, glin_err;  // gp_gl_from_pl / gp_gl_from_float
   DevBuf out_gp, out_site;                                                 // gp_output_records
+  DevBuf lig_a, lig_b, lig_s, lig_cnt;                                     // gp_ligate_overlap / gp_ligate_swap
   std::vector<int32_t> host_nstates;   // K per conditioning set of the current batch
   std::vector<int32_t> impute_np;      // poly sites per conditioning set of the current batch
   std::vector<int32_t> last_phase_nseg;

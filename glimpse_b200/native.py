@@ -23,7 +23,8 @@ EXPORTS = [
     "gp_impute_batch", "gp_rephase_batch", "gp_select", "gp_pbwt_states_get", "gp_sparse_pbwt_get",
     "gp_stage_times", "gp_build_sparse_pbwt", "gp_profile_get", "gp_profile_reset", "gp_stream",
     "gp_impute_one_static",
-    "gp_targets_reset", "gp_gl_from_pl", "gp_gl_from_float", "gp_output_records",
+    "gp_targets_reset", "gp_gl_from_pl", "gp_gl_from_float", "gp_output_records", "gp_ligate_overlap",
+    "gp_ligate_swap",
 ]
 
 
@@ -183,6 +184,29 @@ class Context:
         self._check(self.lib.gp_impute_one_static(self.h, st.size, _p(st, C.c_uint32), _p(hl, C.c_float),
                                                   _p(flat, C.c_uint8), _p(hp, C.c_float)))
         return hp
+
+    def ligate_overlap(self, gta, gtb, swap_prev):
+        """gp_ligate_overlap: gta, gtb (m, n, 2) int32 htslib GT values; swap_prev (n,).
+        Returns swap_next, nmatch, nmism, phaseq."""
+        gta = np.ascontiguousarray(gta, np.int32)
+        gtb = np.ascontiguousarray(gtb, np.int32)
+        m, n = gta.shape[0], gta.shape[1]
+        sp = np.ascontiguousarray(swap_prev, np.uint8)
+        sn = np.zeros(n, np.uint8)
+        nmatch, nmism = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        pq = np.zeros(n, np.float32)
+        self._check(self.lib.gp_ligate_overlap(self.h, n, m, _p(gta, C.c_int32), _p(gtb, C.c_int32), _p(sp, C.c_uint8),
+                                               _p(sn, C.c_uint8), _p(nmatch, C.c_int32), _p(nmism, C.c_int32),
+                                               _p(pq, C.c_float)))
+        return sn, nmatch, nmism, pq
+
+    def ligate_swap(self, gt, swap):
+        """gp_ligate_swap on a copy of gt (m, n, 2) int32; returns the swapped copy."""
+        gt = np.array(gt, np.int32, copy=True, order="C")
+        m, n = gt.shape[0], gt.shape[1]
+        sw = np.ascontiguousarray(swap, np.uint8)
+        self._check(self.lib.gp_ligate_swap(self.h, n, m, _p(gt, C.c_int32), _p(sw, C.c_uint8)))
+        return gt
 
     def output_records(self):
         """gp_output_records after finalize: gp (n, L, 3) float32 as written, and per

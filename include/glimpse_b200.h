@@ -148,6 +148,23 @@ int gp_gp_get(gp_ctx* ctx, float* gp0, float* gp1, float* ds, uint8_t* gt0, uint
  * diploid and 0 < af < 1; the writer omits it for mixed ploidy). */
 int gp_output_records(gp_ctx* ctx, float* gp, float* raf, float* af, float* info);
 
+/* ---- Ligation of consecutive chunks (GLIMPSE2_ligate) ---- */
+
+/* Phase-flip counting over the overlap of two consecutive chunks
+ * (ligater::update_distances and the decision in ligater::scan_overlap,
+ * ligater_algorithm.cpp:108-127,183-205). gta / gtb: htslib GT values (2 int32
+ * per sample) of the m bi-allelic sites present in both chunks, site after site
+ * (m x n x 2). swap_prev: the swap decided for the first chunk. Writes swap_next
+ * (nmatch < nmism), the per-sample counts and the entropy phase quality.
+ * m = 0 returns GP_E_DATA ("Overlap is empty"). */
+int gp_ligate_overlap(gp_ctx* ctx, int32_t n, int32_t m, const int32_t* gta, const int32_t* gtb,
+                      const uint8_t* swap_prev, uint8_t* swap_next, int32_t* nmatch, int32_t* nmism, float* phaseq);
+
+/* ligater::phase_update (ligater_algorithm.cpp:90-106) on m records of a chunk,
+ * in place: for every sample with swap[i], a phased diploid GT becomes
+ * (allele 2 == 1, allele 1 == 1), phased. gt: m x n x 2 htslib GT values. */
+int gp_ligate_swap(gp_ctx* ctx, int32_t n, int32_t m, int32_t* gt, const uint8_t* swap);
+
 /* ---- Call-level entry points (one reference method, batched) ---- */
 
 /* imputation_hmm::computePosteriors(HL, flat, HP) (imputation_hmm.h:59)
