@@ -5,7 +5,7 @@ The init iteration is compared call by call: identical conditioning sets,
 per-site posteriors within 1e-5 and identical sampled/phased haplotypes. Over a
 full run (1 init + burn-in + main) trajectories can part where a uniform falls
 within float rounding of a posterior, so the run is compared by dosage r^2
-against the simulated truth (within 0.002 of the reference)."""
+against the simulated truth (the bar: within 0.002 of the reference's r^2)."""
 import numpy as np
 import pytest
 
