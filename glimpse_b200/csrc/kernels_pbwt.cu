@@ -177,24 +177,25 @@ __device__ __forceinline__ bool any_carrier(const uint32_t* __restrict__ c, int 
 // so the event records a warp reads are the same for all its lanes.
 __global__ void k_event_bits(PbwtSelectArgs a) {
   const int hp = blockIdx.x * blockDim.x + threadIdx.x;
-  const int c = blockIdx.y;
   if (hp >= a.n_haps) return;
   const int nev = a.P.n_events;
   const int t = a.hap_target[hp];
   const uint8_t* H = (a.hap_which[hp] ? a.h1 : a.h0) + (size_t)t * a.L;
   const uint32_t* carry = a.carry + (size_t)hp * a.Wc;
-  uint32_t bits = 0u;
-  const int n = min(32, nev - (c << 5));
-  for (int i = 0; i < n; ++i) {
-    const int e = (c << 5) + i;
-    const int4 r0 = a.P.events[2 * e];
-    const int4 r1 = a.P.events[2 * e + 1];
-    bool b;
-    if (!(r0.x & (1 << 30))) b = H[r0.x] != 0;
-    else b = r1.x > 0 && any_carrier(carry, r0.x & ~(1 << 30), r0.z);
-    if (b) bits |= 1u << i;
+  for (int c = blockIdx.y; c < a.We; c += gridDim.y) {  // gridDim.y is capped at 65535
+    uint32_t bits = 0u;
+    const int n = min(32, nev - (c << 5));
+    for (int i = 0; i < n; ++i) {
+      const int e = (c << 5) + i;
+      const int4 r0 = a.P.events[2 * e];
+      const int4 r1 = a.P.events[2 * e + 1];
+      bool b;
+      if (!(r0.x & (1 << 30))) b = H[r0.x] != 0;
+      else b = r1.x > 0 && any_carrier(carry, r0.x & ~(1 << 30), r0.z);
+      if (b) bits |= 1u << i;
+    }
+    a.ebits[(size_t)hp * a.We + c] = bits;
   }
-  a.ebits[(size_t)hp * a.We + c] = bits;
 }
 
 // Haplotypes per sweep warp. Lane l runs haplotype l % kSweepHaps of its warp's
@@ -480,7 +481,7 @@ __global__ void k_pbwt_union(PbwtSelectArgs a) {
 void launch_pbwt_select(const PbwtSelectArgs& a, cudaStream_t s) {
   k_pbwt_rng<<<1, 32, 0, s>>>(a);
   k_rare_carriers<<<dim3((a.Wc + 127) / 128, a.n_haps), 128, 0, s>>>(a);
-  if (a.We > 0) k_event_bits<<<dim3((a.n_haps + 127) / 128, a.We), 128, 0, s>>>(a);
+  if (a.We > 0) k_event_bits<<<dim3((a.n_haps + 127) / 128, std::min(a.We, 65535)), 128, 0, s>>>(a);
   // Ring of D rank rows, D <= 8, within 96 KB.
   const size_t slot_bytes = (size_t)a.P.R * 4;
   int D = (int)std::min<size_t>(8, (96u << 10) / slot_bytes);
