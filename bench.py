@@ -12,7 +12,14 @@ out inside every timed step.
 
 --impl reference times the reference's own CPU implementation of the path
 (the reference hot-path sources built unmodified as oracle/_ref) on the host
-cores, on a bounded sample of the same workload.
+cores: each step is one complete run (1 init + 5 burn-in + 15 main iterations
+and finalisation) over a fixed subset of the workload's targets (the first
+--subset targets, default one per host thread up to 32), so the work per target
+is the same as in the GPU arm. The GPU arm's line carries the same subset run
+on the GPU beside it (`same_subset`), with the dosage r2 of both.
+
+--case iterations|gl|records runs a small single-stage case for profiler
+captures (python bench.py --case iterations --targets 16 --iterations 2).
 """
 from __future__ import annotations
 
@@ -51,19 +58,16 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def read_traffic_per_cell():
-    """DRAM bytes per imputation cell from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "k_impute_warp_batched.md")
+def read_traffic(kernel):
+    """DRAM bytes per algorithmic unit of a kernel from the committed ncu figures
+    (profiles/traffic.json: one entry per kernel, with the capture it came from)."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(p):
         return None
     with open(p) as f:
-        for line in f:
-            if line.startswith("dram_bytes_per_cell:"):
-                try:
-                    return float(line.split(":", 1)[1].split()[0])
-                except ValueError:
-                    return None
-    return None
+        d = json.load(f)
+    e = d.get(kernel)
+    return None if e is None else float(e["dram_bytes_per_unit"])
 
 
 class ClockSampler:
@@ -133,24 +137,60 @@ def rank_ops(dist, device):
     return barrier, max_over_ranks
 
 
-def cpu_sample(w, n_sample, threads, timed_iters=1):
-    """Reference CPU path on a bounded sample: returns (seconds per burn-in iteration, n)."""
-    from oracle import oracle as O
+def subset(T, n):
+    """The first n targets of a workload's batch (the fixed sample both arms run)."""
     import types
-    T = w.targets
-    idx = np.arange(min(n_sample, T.n))
-    sub = types.SimpleNamespace(n=len(idx), ploidy=T.ploidy[idx], gl=T.gl[idx], flat=T.flat[idx],
-                                truth=T.truth[idx], kpbwt=T.kpbwt[idx])
-    orc = O.RefOracle(w.panel)
-    orc.set_targets(sub)
-    orc.configure(kinit=w.params["kinit"], kpbwt=int(T.kpbwt.max()), kpbwt_target=sub.kpbwt, seed=15052011)
-    orc.iteration(O.STAGE_INIT, 0, threads)
-    times = []
-    for i in range(timed_iters):
+    idx = np.arange(min(n, T.n))
+    return types.SimpleNamespace(n=len(idx), ploidy=T.ploidy[idx], gl=T.gl[idx], flat=T.flat[idx],
+                                 truth=T.truth[idx], kpbwt=T.kpbwt[idx], coverage=T.coverage[idx])
+
+
+def reference_ds(orc, n):
+    """Dosages of a finished reference run: DS = gp1 + 2 gp2 rounded to 1e-3
+    (genotype_writer.cpp:123-126, gp2 = clamp(1 - gp0 - gp1), genotype.h:62-64)."""
+    out = []
+    for t in range(n):
+        g0, g1, _, _, _ = orc.gp(t)
+        g2 = np.clip(np.float32(1.0) - g1 - g0, 0.0, 1.0)
+        out.append(np.round((g1 + np.float32(2.0) * g2) * 1000.0) / 1000.0)
+    return np.stack(out)
+
+
+class ReferenceRun:
+    """The reference's hot path (oracle/_ref: the reference's sources compiled
+    unmodified) on the host cores: one step is one complete run, 1 init +
+    burn-in + main iterations and finalisation, over a fixed subset of the
+    workload's targets, with the reference driver's dynamic assignment of
+    targets to threads and per-thread replay streams."""
+
+    def __init__(self, w, n_targets, threads):
+        from oracle import oracle as O
+        self.O = O
+        self.w = w
+        self.sub = subset(w.targets, n_targets)
+        self.threads = threads
+        self.orc = O.RefOracle(w.panel)
+
+    def step(self):
+        O, sub = self.O, self.sub
+        self.orc.set_targets(sub)
+        self.orc.configure(kinit=self.w.params["kinit"], kpbwt=int(sub.kpbwt.max()), kpbwt_target=sub.kpbwt,
+                           seed=15052011)
         t0 = time.perf_counter()
-        orc.iteration(O.STAGE_BURN, 1 + i, threads)
-        times.append(time.perf_counter() - t0)
-    return times, len(idx)
+        self.orc.run(burnin=BURNIN, main=MAIN, threads=self.threads)
+        return time.perf_counter() - t0
+
+    def dosage_r2(self):
+        return synth.dosage_r2(reference_ds(self.orc, self.sub.n), self.sub.truth.sum(1))
+
+    def sample_text(self, seconds):
+        return (f"{self.sub.n} of the {self.w.targets.n} targets (the first {self.sub.n}), one complete run per "
+                f"step (1 init + {BURNIN} burn-in + {MAIN} main iterations and finalisation, {seconds:.1f} s) on "
+                f"{self.threads} threads (per-thread replay RNG); samples/s = targets / run time")
+
+
+def default_subset(threads):
+    return max(1, min(threads, 32))
 
 
 def run_reference(args):
@@ -167,19 +207,20 @@ def run_reference(args):
         return 0
     w = synth.workload(args.config, seed=1)
     threads = os.cpu_count() or 1
-    n_sample = threads
-    times, n = cpu_sample(w, n_sample, threads, timed_iters=args.warmup + args.steps)
-    timed = times[args.warmup:]
-    t_iter = sum(timed) / len(timed)
-    value = n / (N_ITER * t_iter)
-    sample = (f"{n} of the {w.targets.n} targets, one burn-in iteration per step on {threads} threads "
-              f"(per-thread replay RNG); samples/s = targets / ({N_ITER} x iteration time)")
+    ref = ReferenceRun(w, args.subset or default_subset(threads), threads)
+    for _ in range(args.warmup):
+        ref.step()
+    times = [ref.step() for _ in range(args.steps)]
+    t_run = sum(times) / len(times)
+    value = ref.sub.n / t_run
     line = {"metric": METRIC, "value": value, "unit": "samples/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_iter * 1000.0, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_run * 1000.0, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "parallelism": f"{threads} host threads"},
+            "config": {"workload": WORKLOAD, "parallelism": f"{threads} host threads",
+                       "targets_timed": ref.sub.n},
+            "dosage_r2": ref.dosage_r2(),
             "cpu_baseline": {"value": value, "unit": "samples/s", "cores": threads, "kind": "reference",
-                             "sample": sample},
+                             "sample": ref.sample_text(t_run)},
             "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -266,12 +307,27 @@ def run_ours(args):
     peak, peak_kind = load_peaks()
     achieved = prof["impute_bytes"] / (prof["impute_ms"] / 1000.0) / 1e9 if prof["impute_ms"] > 0 else 0.0
     per_launch_cells = prof["impute_cells"] / max(1, prof["impute_launches"])
-    tpc = read_traffic_per_cell()
+    tpc = read_traffic("k_impute_warp")
     roofline = {"bound": "hbm", "kernel": "k_impute_warp (imputation forward-backward)", "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                 "algorithmic_bytes_per_cell": 8.25, "cells_per_launch": per_launch_cells,
                 "launch_ms": prof["impute_ms"] / max(1, prof["impute_launches"]),
                 "traffic": (tpc * per_launch_cells) if tpc is not None else None}
+    # Phasing (k_phase) is bound by its per-site dependent chain, not by HBM: its
+    # messages live in registers. Reported against the FP32 issue rate at the
+    # sampled clock: 148 SMs x 128 lanes x 2 flop per FMA.
+    sm_mhz = clk.get("sm_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    phase_cells_s = prof["phase_cells"] / (prof["phase_ms"] / 1000.0) if prof["phase_ms"] > 0 else 0.0
+    phase = {"kernel": "k_phase (phasing backward + forward with diplotype sampling)", "bound": "latency",
+             "cells_per_s": phase_cells_s, "launch_ms": prof["phase_ms"] / max(1, prof["phase_launches"]),
+             "share_of_step": prof["phase_ms"] / args.steps / ms, "flops_per_cell": 4,
+             "fp32_tflops": phase_cells_s * 4 / 1e12, "fp32_peak_tflops": fp32_peak,
+             "fp32_frac": phase_cells_s * 4 / 1e12 / fp32_peak,
+             "cell": "(VAR site, state, hypothesis) of one pass; 4 flop: transition fma, emission mul, sum add"}
+    select = {"kernels": "k_pbwt_sweep + k_pbwt_union + conditioning-set build", "bound": "latency",
+              "share_of_step": prof["select_ms"] / args.steps / ms,
+              "ms_per_iteration": prof["select_ms"] / args.steps / N_ITER}
     hmm_cells = (prof["impute_cells"] + prof["phase_cells"]) / (args.steps)
     line = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -284,20 +340,97 @@ def run_ours(args):
             "gpu_launches": int(prof["kernel_launches"]),
             "clocks": clk,
             "roofline": roofline,
+            "phasing": phase,
+            "selection": select,
             "e2e": {"value": e2e_value, "unit": "samples/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # The same fixed subset on both sides: a complete run of the first
+        # targets, on the GPU (device time) and on the host cores (reference).
         threads = os.cpu_count() or 1
-        times, ns = cpu_sample(w, threads, threads, timed_iters=1)
-        cpu_value = ns / (N_ITER * times[0])
+        sub = subset(T, args.subset or default_subset(threads))
+        ctx.set_targets(sub, kpbwt=sub.kpbwt)
+        for _ in range(max(1, min(args.warmup, 3))):
+            device_step()
+        reps = max(1, min(args.steps, 3))
+        torch.cuda.synchronize()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(reps):
+            device_step()
+        s1.record(stream)
+        torch.cuda.synchronize()
+        ms_sub = s0.elapsed_time(s1) / reps
+        _, _, ds_sub, _, _ = ctx.gp()
+        ref = ReferenceRun(w, sub.n, threads)
+        t_ref = ref.step()
+        cpu_value = sub.n / t_ref
         line["cpu_baseline"] = {"value": cpu_value, "unit": "samples/s", "cores": threads, "kind": "reference",
-                                "sample": f"{ns} targets, one burn-in iteration on {threads} threads "
-                                          f"({times[0]:.1f} s); samples/s = targets / ({N_ITER} x iteration time)"}
+                                "sample": ref.sample_text(t_ref)}
+        line["same_subset"] = {"targets": sub.n, "gpu_samples_per_s": sub.n / (ms_sub / 1000.0),
+                               "gpu_ms_per_run": ms_sub, "reference_samples_per_s": cpu_value,
+                               "reference_cores": threads,
+                               "gpu_dosage_r2": synth.dosage_r2(ds_sub, sub.truth.sum(1)),
+                               "reference_dosage_r2": ref.dosage_r2()}
     if rank == 0:
         print(json.dumps(line))
     ctx.close()
     if dist is not None:
         dist.destroy_process_group()
+    return 0
+
+
+def run_case(args):
+    """Small cases of single stages, for profiler captures and quick timings
+    (not bench lines): `iterations` runs Gibbs iterations of a workload with a
+    reduced batch; `gl` times the target GL input; `records` the output epilogue."""
+    from glimpse_b200 import native
+    if args.case == "iterations":
+        w = synth.workload(args.config, seed=1, n_targets=args.targets)
+        T = w.targets
+        ctx = native.Context(w.panel, kinit=w.params["kinit"], kpbwt=int(T.kpbwt.max()))
+        ctx.set_targets(T, kpbwt=T.kpbwt)
+        for it in range(args.iterations):
+            t0 = time.perf_counter()
+            ctx.iteration(0 if it == 0 else 1, it)
+            print(f"iteration {it}: {1000 * (time.perf_counter() - t0):.1f} ms, stages (ms) "
+                  f"{ctx.stage_times().round(1)}")
+        print(ctx.profile())
+        ctx.close()
+    elif args.case == "gl":
+        n, L = args.targets, 150_000
+        rng = np.random.default_rng(1)
+        if args.fmt == "PL":
+            src = rng.integers(0, 300, size=(L, n, 3), dtype=np.int32)
+        else:
+            src = (-rng.uniform(0, 30, size=(L, n, 3))).astype(np.float32)
+        ploidy = np.full(n, 2, np.int32)
+        # any panel serves: the conversion does not read it
+        w = synth.make_panel_and_targets(600, 4000, 0.4, 0.5, 1, ("uniform", 0.5, 2.0), ("uniform", 80, 300),
+                                         seed=7, sparse_maf=0.01, lq_frac=0.02, alt_major_frac=0.1)
+        ctx = native.Context(w.panel)
+        times = []
+        for _ in range(args.reps + 1):
+            t0 = time.perf_counter()
+            ctx.gl_from_format(args.fmt, src, ploidy)
+            times.append(time.perf_counter() - t0)
+        t = float(np.median(times[1:]))
+        print(f"{args.fmt}: {n} targets x {L} sites, {1e3 * t:.1f} ms per call (median of {args.reps})")
+        ctx.close()
+    elif args.case == "records":
+        w = synth.workload(args.config, seed=1, n_targets=args.targets)
+        T = w.targets
+        ctx = native.Context(w.panel, kinit=w.params["kinit"], kpbwt=int(T.kpbwt.max()))
+        ctx.set_targets(T, kpbwt=T.kpbwt)
+        ctx.run(0, 1)
+        times = []
+        for _ in range(args.reps + 1):
+            t0 = time.perf_counter()
+            ctx.output_records()
+            times.append(time.perf_counter() - t0)
+        print(f"output records: {T.n} targets, {1e3 * float(np.median(times[1:])):.1f} ms per call")
+        ctx.close()
     return 0
 
 
@@ -309,7 +442,17 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", default="batched")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--subset", type=int, default=0,
+                    help="targets of the fixed subset both arms run completely (default: host threads, at most 32)")
+    ap.add_argument("--case", choices=["iterations", "gl", "records"], default=None,
+                    help="run a small single-stage case (for profiler captures) instead of the bench")
+    ap.add_argument("--targets", type=int, default=16)
+    ap.add_argument("--iterations", type=int, default=2)
+    ap.add_argument("--fmt", choices=["PL", "GL"], default="PL")
+    ap.add_argument("--reps", type=int, default=5)
     args = ap.parse_args()
+    if args.case:
+        return run_case(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

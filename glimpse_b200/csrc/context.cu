@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <numeric>
@@ -16,19 +17,23 @@ namespace {
 
 // HvarRef (row = common site, MSB-first bytes, bitmatrix.h:89-119) to
 // haplotype-major 32-bit words: refT[h][w] bit i = allele of h at common row 32w+i.
+// Thread x is haplotype blockIdx.x * blockDim.x + x; the words run over blockIdx.y
+// in steps of gridDim.y, which the launch caps at 65535 (panels with more than
+// 2,097,120 common sites need more than one word per block row).
 __global__ void k_transpose_panel(const uint8_t* __restrict__ hvar, int n_com, int stride, int N, int W,
                                   uint32_t* __restrict__ refT) {
   const int h = blockIdx.x * blockDim.x + threadIdx.x;
-  const int wi = blockIdx.y;
   if (h >= N) return;
-  uint32_t word = 0;
-  const int r0 = wi * 32;
-  const int n = min(32, n_com - r0);
-  for (int i = 0; i < n; ++i) {
-    const uint8_t byte = hvar[(size_t)(r0 + i) * stride + (h >> 3)];
-    word |= (uint32_t)((byte >> (7 - (h & 7))) & 1) << i;
+  for (int wi = blockIdx.y; wi < W; wi += gridDim.y) {
+    uint32_t word = 0;
+    const int r0 = wi * 32;
+    const int n = min(32, n_com - r0);
+    for (int i = 0; i < n; ++i) {
+      const uint8_t byte = hvar[(size_t)(r0 + i) * stride + (h >> 3)];
+      word |= (uint32_t)((byte >> (7 - (h & 7))) & 1) << i;
+    }
+    refT[(size_t)h * W + wi] = word;
   }
-  refT[(size_t)h * W + wi] = word;
 }
 
 }  // namespace
@@ -183,9 +188,10 @@ int Context::create_panel(const gp_panel_desc& d) {
     if ((e = cudaMalloc(&dh, host.hvar.size())) != cudaSuccess) return cuda_fail(e, "hvar staging");
     e = cudaMemcpy(dh, host.hvar.data(), host.hvar.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
-      dim3 g((N + 255) / 256, P.W);
+      dim3 g((N + 255) / 256, std::min(P.W, grid_y_cap));
       k_transpose_panel<<<g, 256, 0, stream>>>(dh, nc, stride, N, P.W, P.refT);
-      e = cudaStreamSynchronize(stream);
+      e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     }
     cudaFree(dh);
     if (e != cudaSuccess) return cuda_fail(e, "panel transpose");
@@ -230,6 +236,7 @@ Context::~Context() {
   glin_err.release();
   out_gp.release(); out_site.release();
   lig_a.release(); lig_b.release(); lig_s.release(); lig_cnt.release();
+  if (phase_err_host) cudaFreeHost(phase_err_host);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -322,12 +329,29 @@ int Context::run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
   const int J = impute_groups(Kmax);
   cudaEvent_t ea;
   prof_begin(ea);
-  if (launch_impute_warp(1, J, mc, w, d_hp, stream) != GP_OK || launch_impute_warp(2, J, mc, w, d_hp, stream) != GP_OK)
-    return (fail(GP_E_ARG, "imputation: too many states"), GP_E_ARG);
+  int lrc = launch_impute_warp(1, J, mc, w, d_hp, stream);
+  if (lrc == GP_OK) lrc = launch_impute_warp(2, J, mc, w, d_hp, stream);
+  if (lrc == GP_E_CUDA) return cuda_fail(cudaGetLastError(), "imputation: shared-memory attribute");
+  if (lrc != GP_OK) return (fail(GP_E_ARG, "imputation: too many states"), GP_E_ARG);
   prof_end(ea, 0, cells);
   launch_impute_finish(panel, mc, w, d_hl, d_flat, d_hp, stream);
   prof.kernel_launches += 4;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "imputation launch");
+  return GP_OK;
+}
+
+// After a synchronisation that follows run_phase: GP_E_DATA naming the first
+// target whose diplotype draw saw a NaN, infinite or sub-normal sum. The draw
+// keeps the previous diplotype there and the run is otherwise complete; the
+// reference stops on an assertion (phasing_hmm.cpp:175).
+int Context::check_phase_errors() {
+  const int n = phase_err_n;
+  phase_err_n = 0;
+  for (int b = 0; b < n; ++b)
+    if (phase_err_host[b])
+      return (fail(GP_E_DATA, "phasing: invalid diplotype probabilities (NaN, infinite or zero sum) for target " +
+                                  std::to_string(phase_err_ids[b])),
+              GP_E_DATA);
   return GP_OK;
 }
 
@@ -430,6 +454,18 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
                    w.npoly.as<int32_t>(), L, panel.cm, V, S, mc, cfg.seed, iteration, d_target_ids, stream) != GP_OK)
     return (fail(GP_E_ARG, "phasing: too many states"), GP_E_ARG);
   prof_end(ea, 1, pcells);
+  // SAMPLE_DIP's invalid-sum flags (the reference asserts there, phasing_hmm.cpp:175).
+  if (phase_err_cap < nb) {
+    if (phase_err_host) cudaFreeHost(phase_err_host);
+    phase_err_host = nullptr;
+    phase_err_cap = 0;
+    if ((e = cudaMallocHost(&phase_err_host, (size_t)nb * 4)) != cudaSuccess) return cuda_fail(e, "alloc err flags");
+    phase_err_cap = nb;
+  }
+  cudaMemcpyAsync(phase_err_host, S.err, (size_t)nb * 4, cudaMemcpyDeviceToHost, stream);
+  phase_err_n = nb;
+  phase_err_ids.resize(nb);
+  for (int b = 0; b < nb; ++b) phase_err_ids[b] = tsel_host.empty() ? b : tsel_host[b];
   launch_phase_writeback(d_tsel, nb, w.poly.as<int32_t>(), w.polyidx.as<int32_t>(), L, V, S, mc, cfg.seed, iteration,
                          d_target_ids, d_h0, d_h1, stream);
   prof.kernel_launches += 4;
@@ -467,6 +503,12 @@ int gp_ctx_create(const gp_panel_desc* panel, const gp_config* cfg, gp_ctx** out
   std::unique_ptr<Context> c(new (std::nothrow) Context());
   if (!c) return GP_E_NOMEM;
   c->cfg = *cfg;
+  if (const char* cap = std::getenv("GLIMPSE_B200_GRID_Y_CAP")) {
+    // Lowers the largest gridDim.y of the launches that loop over a second grid
+    // dimension (tests use it to run those loops on small panels).
+    const long v = std::strtol(cap, nullptr, 10);
+    if (v >= 1 && v <= 65535) c->grid_y_cap = (int)v;
+  }
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return GP_E_CUDA;
   int rc = c->create_panel(*panel);
   if (rc != GP_OK) {
@@ -491,7 +533,8 @@ int gp_impute_batch(gp_ctx* ctx, int32_t n, const int64_t* states_off, const uin
                     const uint8_t* flat, float* hp) {
   if (!ctx) return GP_E_ARG;
   Context& c = *reinterpret_cast<Context*>(ctx);
-  if (n <= 0 || !states_off || !states || !hl || !flat || !hp) return (c.fail(GP_E_ARG, "impute: bad argument"), GP_E_ARG);
+  if (n <= 0 || n > GP_MAX_BATCH || !states_off || !states || !hl || !flat || !hp)
+    return (c.fail(GP_E_ARG, "impute: bad argument"), GP_E_ARG);
   const int L = c.panel.L;
   std::vector<int64_t> off(states_off, states_off + n + 1);
   std::vector<uint32_t> st(states, states + off[n]);
@@ -516,7 +559,8 @@ int gp_rephase_batch(gp_ctx* ctx, int32_t n, const int64_t* states_off, const ui
                      uint8_t* h1, const uint8_t* flat, int32_t iteration, const int32_t* target_ids) {
   if (!ctx) return GP_E_ARG;
   Context& c = *reinterpret_cast<Context*>(ctx);
-  if (n <= 0 || !states_off || !states || !h0 || !h1 || !flat) return (c.fail(GP_E_ARG, "rephase: bad argument"), GP_E_ARG);
+  if (n <= 0 || n > GP_MAX_BATCH || !states_off || !states || !h0 || !h1 || !flat)
+    return (c.fail(GP_E_ARG, "rephase: bad argument"), GP_E_ARG);
   const int L = c.panel.L;
   std::vector<int64_t> off(states_off, states_off + n + 1);
   std::vector<uint32_t> st(states, states + off[n]);
@@ -544,7 +588,8 @@ int gp_rephase_batch(gp_ctx* ctx, int32_t n, const int64_t* states_off, const ui
   cudaMemcpyAsync(h1, bh1.ptr, (size_t)n * L, cudaMemcpyDeviceToHost, c.stream);
   if ((e = cudaStreamSynchronize(c.stream)) != cudaSuccess) return c.cuda_fail(e, "rephase");
   c.prof_resolve();
-  return GP_OK;
+  for (int b = 0; b < n; ++b) c.phase_err_ids[b] = ids[b];
+  return c.check_phase_errors();
 }
 
 int gp_sparse_pbwt_get(gp_ctx* ctx, uint8_t* ypacked, int64_t* ypacked_len, int64_t* asmall_off,

@@ -64,6 +64,12 @@ struct Context {
   std::vector<int32_t> host_nstates;   // K per conditioning set of the current batch
   std::vector<int32_t> impute_np;      // poly sites per conditioning set of the current batch
   std::vector<int32_t> last_phase_nseg;
+  // Per-target diplotype-draw error flags of the last phasing launch, copied to
+  // pinned host memory on the stream and read after the caller's synchronisation.
+  int32_t* phase_err_host = nullptr;
+  int phase_err_cap = 0, phase_err_n = 0;
+  std::vector<int32_t> phase_err_ids;  // target reported for each flag
+  int check_phase_errors();
   TargetWork tw;
   SparsePbwt sparse;
   DevPbwt pbwt;
@@ -71,6 +77,7 @@ struct Context {
   float pbwt_modulo = 0.1f;
   std::vector<int32_t> pbwt_grp;
   int tw_push_cap = 4096;
+  int grid_y_cap = 65535;  // largest gridDim.y of the launches that loop over it (GLIMPSE_B200_GRID_Y_CAP)
   float stage_ms[5] = {0, 0, 0, 0, 0};
   // profiling: events around the hot kernels, resolved at the next host sync
   struct ProfEv {

@@ -164,8 +164,17 @@ int Context::iteration(int stage, int iteration) {
   if (T.n <= 0) return (fail(GP_E_STATE, "no targets"), GP_E_STATE);
   if (stage < GP_STAGE_INIT || stage > GP_STAGE_MAIN) return (fail(GP_E_ARG, "bad stage"), GP_E_ARG);
   const int n = T.n, L = panel.L;
-  cudaEvent_t ev[6];
-  for (auto& x : ev) cudaEventCreate(&x);
+  struct Events {  // destroyed on every return path
+    cudaEvent_t ev[6] = {};
+    ~Events() {
+      for (auto& x : ev)
+        if (x) cudaEventDestroy(x);
+    }
+  } evs;
+  cudaEvent_t* ev = evs.ev;
+  phase_err_n = 0;
+  for (int i = 0; i < 6; ++i)
+    if (cudaEventCreate(&ev[i]) != cudaSuccess) return cuda_fail(cudaGetLastError(), "iteration events");
   cudaEventRecord(ev[0], stream);
   int Kp = 0;
   int rc = select_states(stage, iteration, Kp);
@@ -214,10 +223,9 @@ int Context::iteration(int stage, int iteration) {
   if (e != cudaSuccess) return cuda_fail(e, "iteration");
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "iteration launch");
   for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&stage_ms[i], ev[i], ev[i + 1]);
-  for (auto& x : ev) cudaEventDestroy(x);
   prof.select_ms += stage_ms[0];
   prof_resolve();
-  return GP_OK;
+  return check_phase_errors();
 }
 
 int Context::finalize() {
@@ -246,6 +254,9 @@ int gp_targets_set(gp_ctx* ctx, int32_t n, const uint8_t* gl, const uint8_t* fla
                    const int32_t* kpbwt) {
   if (!ctx) return GP_E_ARG;
   if (n <= 0 || !gl || !flat || !ploidy) return (C_(ctx)->fail(GP_E_ARG, "targets: bad argument"), GP_E_ARG);
+  if (n > GP_MAX_TARGETS)
+    return (C_(ctx)->fail(GP_E_ARG, "targets: more than " + std::to_string(GP_MAX_TARGETS) + " targets per context"),
+            GP_E_ARG);
   return C_(ctx)->set_targets(n, gl, flat, ploidy, kpbwt);
 }
 
@@ -342,6 +353,21 @@ int gp_gp_get(gp_ctx* ctx, float* gp0, float* gp1, float* ds, uint8_t* gt0, uint
   if (gt1) cudaMemcpyAsync(gt1, c.tw.gt1.ptr, nL, cudaMemcpyDeviceToHost, c.stream);
   cudaError_t e = cudaStreamSynchronize(c.stream);
   return e == cudaSuccess ? GP_OK : c.cuda_fail(e, "gp_get");
+}
+
+int gp_gp_accum_get(gp_ctx* ctx, int32_t target, float* gp0, float* gp1, uint8_t* flags) {
+  if (!ctx || !gp0 || !gp1 || !flags) return GP_E_ARG;
+  Context& c = *C_(ctx);
+  if (target < 0 || target >= c.tw.n) return (c.fail(GP_E_ARG, "target out of range"), GP_E_ARG);
+  const size_t L = c.panel.L, o = (size_t)target * L;
+  cudaMemcpyAsync(gp0, c.tw.gp0.as<float>() + o, L * 4, cudaMemcpyDeviceToHost, c.stream);
+  cudaMemcpyAsync(gp1, c.tw.gp1.as<float>() + o, L * 4, cudaMemcpyDeviceToHost, c.stream);
+  cudaMemcpyAsync(flags, c.tw.gpflags.as<uint8_t>() + o, L, cudaMemcpyDeviceToHost, c.stream);
+  cudaError_t e = cudaStreamSynchronize(c.stream);
+  if (e != cudaSuccess) return c.cuda_fail(e, "gp_accum_get");
+  for (size_t l = 0; l < L; ++l)
+    if (!(flags[l] & 1)) gp0[l] = gp1[l] = 0.0f;
+  return GP_OK;
 }
 
 int gp_targets_reset(gp_ctx* ctx) {

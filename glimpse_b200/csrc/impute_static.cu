@@ -11,8 +11,13 @@
 //     would pay for cudaMalloc, and cudaFree waits for the whole device,
 //     serialising it against every other stream in the process.
 // For them this entry point takes its scratch from g_impute_scratch below. The
-// region is fixed at kStaticScratchBytes per device; a call whose layout does
-// not fit is refused with GP_E_ARG before any work is queued.
+// region is fixed at kStaticScratchBytes per device. The per-site buffers are
+// sized on all L sites, and a call whose per-site buffers do not fit is refused
+// with GP_E_ARG before any work is queued. The forward-backward store takes the
+// rest of the region; it needs (polymorphic sites of the conditioning set) x
+// (row stride) x 4 bytes, which is known only once the conditioning set is
+// built on the device, so a call whose store does not fit is refused with
+// GP_E_ARG after that step and before the HMM runs.
 //
 // The region's address is looked up once per device, the first time the entry
 // is called with that device current (cudaGetSymbolAddress); that first call
@@ -25,6 +30,8 @@
 // where their buffers live differs.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "context.h"
 #include "internal.h"
 
@@ -36,19 +43,18 @@ constexpr int kMaxDevices = 64;
 
 __device__ __align__(256) unsigned char g_impute_scratch[kStaticScratchBytes];
 
-unsigned char* g_scratch_addr[kMaxDevices] = {};
+std::atomic<unsigned char*> g_scratch_addr[kMaxDevices] = {};
 
 size_t round256(size_t x) { return (x + 255) & ~size_t(255); }
 
 // Byte offsets of every buffer of a one-haplotype imputation inside the region.
+// The per-site buffers are sized on all L sites; the forward-backward store
+// starts at `alpha` and may use the region up to its end.
 struct StaticLayout {
-  size_t states, nstates, mark, polyidx, poly, npoly, hvar, em, tr, fl, alpha_off, split, split_scr, alpha, hl, hp,
-      flat, total;
+  size_t states, nstates, mark, polyidx, poly, npoly, hvar, em, tr, fl, alpha_off, split, split_scr, hl, hp, flat,
+      alpha;
 };
 
-// Upper bounds: the poly-site count is at most L (the exact count is known only
-// after compaction on the device), so the store is sized L x Ks (Ks: its row
-// stride in padded state coordinates).
 StaticLayout static_layout(int L, int Kp, int Ks) {
   const int WB = (L + 31) / 32;
   StaticLayout s{};
@@ -71,11 +77,10 @@ StaticLayout static_layout(int L, int Kp, int Ks) {
   s.alpha_off = take(8);
   s.split = take(4);
   s.split_scr = take((size_t)(4 + Ks) * 4);
-  s.alpha = take((size_t)L * Ks * 4);
   s.hl = take((size_t)L * 2 * 4);
   s.hp = take((size_t)L * 2 * 4);
   s.flat = take((size_t)L);
-  s.total = o;
+  s.alpha = o;
   return s;
 }
 
@@ -105,11 +110,12 @@ extern "C" int gp_impute_one_static(gp_ctx* ctx, int32_t k, const uint32_t* stat
   const int Kp = (k + 31) / 32 * 32;
   const int Ks = gp::impute_store_stride(k);
   const gp::StaticLayout lay = gp::static_layout(L, Kp, Ks);
-  if (lay.total > gp::kStaticScratchBytes)
-    return (c.fail(GP_E_ARG, "impute_one_static: " + std::to_string(L) + " sites x " + std::to_string(k) +
-                                 " states need " + std::to_string(lay.total >> 20) +
+  if (lay.alpha + (size_t)Ks * 4 * 32 > gp::kStaticScratchBytes)
+    return (c.fail(GP_E_ARG, "impute_one_static: the per-site buffers of " + std::to_string(L) + " sites x " +
+                                 std::to_string(k) + " states need " + std::to_string(lay.alpha >> 20) +
                                  " MiB of scratch, above the fixed 64 MiB"),
             GP_E_ARG);
+  const size_t store_cap = gp::kStaticScratchBytes - lay.alpha;
   const int dev = c.cfg.device;
   if (dev < 0 || dev >= gp::kMaxDevices) return (c.fail(GP_E_ARG, "impute_one_static: device ordinal"), GP_E_ARG);
 
@@ -122,13 +128,14 @@ extern "C" int gp_impute_one_static(gp_ctx* ctx, int32_t k, const uint32_t* stat
     return rc;
   };
   // Per-device set-up: the region's device address, looked up with the device current.
-  if (!gp::g_scratch_addr[dev]) {
+  unsigned char* base = gp::g_scratch_addr[dev].load(std::memory_order_acquire);
+  if (!base) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, gp::g_impute_scratch);
     if (e != cudaSuccess || !p) return finish(c.cuda_fail(e, "impute_one_static: scratch symbol address"));
-    gp::g_scratch_addr[dev] = static_cast<unsigned char*>(p);
+    base = static_cast<unsigned char*>(p);
+    gp::g_scratch_addr[dev].store(base, std::memory_order_release);
   }
-  unsigned char* base = gp::g_scratch_addr[dev];
 
   gp::ImputeWork w;
   w.n = 1;
@@ -149,7 +156,7 @@ extern "C" int gp_impute_one_static(gp_ctx* ctx, int32_t k, const uint32_t* stat
   gp::point(w.alpha_off, base, lay.alpha_off, 8);
   gp::point(w.split, base, lay.split, 4);
   gp::point(w.split_scr, base, lay.split_scr, (size_t)(4 + Ks) * 4);
-  gp::point(w.alpha, base, lay.alpha, (size_t)L * Ks * 4);
+  gp::point(w.alpha, base, lay.alpha, store_cap);
   gp::point(w.hl, base, lay.hl, (size_t)L * 8);
   gp::point(w.hp, base, lay.hp, (size_t)L * 8);
   gp::point(w.flat, base, lay.flat, L);
@@ -169,14 +176,22 @@ extern "C" int gp_impute_one_static(gp_ctx* ctx, int32_t k, const uint32_t* stat
   int32_t np = 0;
   cudaMemcpyAsync(&np, w.npoly.ptr, 4, cudaMemcpyDeviceToHost, s);
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return finish(c.cuda_fail(e, "impute_one_static: conditioning set"));
+  if ((size_t)np * Ks * 4 > store_cap)
+    return finish((c.fail(GP_E_ARG, "impute_one_static: " + std::to_string(np) + " polymorphic sites x " +
+                                        std::to_string(k) + " states need a " +
+                                        std::to_string(((size_t)np * Ks * 4) >> 20) +
+                                        " MiB forward-backward store; the fixed 64 MiB region has " +
+                                        std::to_string(store_cap >> 20) + " MiB left for it"),
+                   GP_E_ARG));
   const int32_t split = (np / 2) & ~31;  // forward/backward meeting point, a multiple of 32
   cudaMemcpyAsync(w.alpha_off.ptr, &zero64, 8, cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(w.split.ptr, &split, 4, cudaMemcpyHostToDevice, s);
   gp::launch_site_records(c.panel, c.mc, w, w.hl.as<float>(), w.flat.as<uint8_t>(), s);
   const int J = gp::impute_groups(k);
-  if (gp::launch_impute_warp(1, J, c.mc, w, w.hp.as<float>(), s) != GP_OK ||
-      gp::launch_impute_warp(2, J, c.mc, w, w.hp.as<float>(), s) != GP_OK)
-    return finish((c.fail(GP_E_ARG, "impute_one_static: too many states"), GP_E_ARG));
+  int lrc = gp::launch_impute_warp(1, J, c.mc, w, w.hp.as<float>(), s);
+  if (lrc == GP_OK) lrc = gp::launch_impute_warp(2, J, c.mc, w, w.hp.as<float>(), s);
+  if (lrc == GP_E_CUDA) return finish(c.cuda_fail(cudaGetLastError(), "impute_one_static: shared-memory attribute"));
+  if (lrc != GP_OK) return finish((c.fail(GP_E_ARG, "impute_one_static: too many states"), GP_E_ARG));
   gp::launch_impute_finish(c.panel, c.mc, w, w.hl.as<float>(), w.flat.as<uint8_t>(), w.hp.as<float>(), s);
   c.prof.kernel_launches += 9;
   cudaMemcpyAsync(hp, w.hp.ptr, (size_t)L * 8, cudaMemcpyDeviceToHost, s);

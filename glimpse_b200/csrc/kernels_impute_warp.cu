@@ -504,12 +504,12 @@ template <int J, bool POST>
 static int launch_chains(const ChainArgs& a, cudaStream_t s) {
   constexpr int W = kWarpsPerChain;
   const size_t sm = impute_warp_smem(J);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_impute_warp<J, W, POST>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
   if (sm > 200 * 1024) return GP_E_ARG;
+  // The attribute is per device (contexts may sit on different devices);
+  // setting it at every launch is cheap.
+  if (cudaFuncSetAttribute(k_impute_warp<J, W, POST>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) !=
+      cudaSuccess)
+    return GP_E_CUDA;
   const dim3 g((a.nchains + kChainsPerCta - 1) / kChainsPerCta);
   k_impute_warp<J, W, POST><<<g, 32 * W * kChainsPerCta, sm, s>>>(a);
   return GP_OK;

@@ -182,7 +182,7 @@ __global__ void k_event_bits(PbwtSelectArgs a) {
   const int t = a.hap_target[hp];
   const uint8_t* H = (a.hap_which[hp] ? a.h1 : a.h0) + (size_t)t * a.L;
   const uint32_t* carry = a.carry + (size_t)hp * a.Wc;
-  for (int c = blockIdx.y; c < a.We; c += gridDim.y) {  // gridDim.y is capped at 65535
+  for (int c = blockIdx.y; c < a.We; c += gridDim.y) {  // gridDim.y is capped at grid_y_cap <= 65535
     uint32_t bits = 0u;
     const int n = min(32, nev - (c << 5));
     for (int i = 0; i < n; ++i) {
@@ -481,17 +481,15 @@ __global__ void k_pbwt_union(PbwtSelectArgs a) {
 void launch_pbwt_select(const PbwtSelectArgs& a, cudaStream_t s) {
   k_pbwt_rng<<<1, 32, 0, s>>>(a);
   k_rare_carriers<<<dim3((a.Wc + 127) / 128, a.n_haps), 128, 0, s>>>(a);
-  if (a.We > 0) k_event_bits<<<dim3((a.n_haps + 127) / 128, std::min(a.We, 65535)), 128, 0, s>>>(a);
+  const int ycap = std::max(1, std::min(a.grid_y_cap, 65535));
+  if (a.We > 0) k_event_bits<<<dim3((a.n_haps + 127) / 128, std::min(a.We, ycap)), 128, 0, s>>>(a);
   // Ring of D rank rows, D <= 8, within 96 KB.
   const size_t slot_bytes = (size_t)a.P.R * 4;
   int D = (int)std::min<size_t>(8, (96u << 10) / slot_bytes);
   if (D < 2) D = 0;
   const size_t smem = (size_t)D * slot_bytes + 2 * 32 * 2 * 16 + (size_t)a.depth * 32 * 4;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_pbwt_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 << 10);
-    attr = true;
-  }
+  // The attribute is per device; setting it at every launch is cheap.
+  if (smem > (48u << 10)) cudaFuncSetAttribute(k_pbwt_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 << 10);
   k_pbwt_sweep<<<(a.n_haps + kSweepHaps - 1) / kSweepHaps, 32, smem, s>>>(a, D);
   k_pbwt_union<<<(a.n_targets + 63) / 64, 64, 0, s>>>(a);
 }

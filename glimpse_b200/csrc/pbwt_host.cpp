@@ -519,6 +519,7 @@ int Context::pbwt_select_states(int stage, int iteration, int Kp) {
     if (ec != cudaSuccess) return cuda_fail(ec, "alloc event bits");
   }
   a.ebits = T.ebits.as<uint32_t>();
+  a.grid_y_cap = grid_y_cap;
   a.start_idx = T.start_idx.as<int32_t>();
   a.tar_hap = T.tar_hap.as<uint8_t>();
   a.push_key = T.push_key.as<uint32_t>();

@@ -87,6 +87,7 @@ struct PbwtSelectArgs {
                               // haplotype's allele at that HQ common site, or for a run of rare sites, whether it
                               // carries a non-major allele at a non-LQ site of the run
   int We;                     // ceil(n_events / 32)
+  int grid_y_cap;             // largest gridDim.y of the event-bit launch (65535, the hardware limit, by default)
   int32_t* start_idx;         // [n_haps] random pbwt_index
   uint8_t* tar_hap;           // [n_haps] persistent across iterations
   uint32_t* push_key;         // [n_haps][depth][cap]

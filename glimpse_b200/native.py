@@ -24,7 +24,7 @@ EXPORTS = [
     "gp_stage_times", "gp_build_sparse_pbwt", "gp_profile_get", "gp_profile_reset", "gp_stream",
     "gp_impute_one_static",
     "gp_targets_reset", "gp_gl_from_pl", "gp_gl_from_float", "gp_output_records", "gp_ligate_overlap",
-    "gp_ligate_swap",
+    "gp_ligate_swap", "gp_gp_accum_get",
 ]
 
 
@@ -316,6 +316,14 @@ class Context:
         self._check(self.lib.gp_gp_get(self.h, _p(gp0, C.c_float), _p(gp1, C.c_float), _p(ds, C.c_float),
                                        _p(gt0, C.c_uint8), _p(gt1, C.c_uint8)))
         return gp0, gp1, ds, gt0, gt1
+
+    def gp_accum(self, target):
+        """gp_gp_accum_get: (gp0, gp1, flags) of one target, dense over the sites."""
+        gp0, gp1 = np.zeros(self.L, np.float32), np.zeros(self.L, np.float32)
+        fl = np.zeros(self.L, np.uint8)
+        self._check(self.lib.gp_gp_accum_get(self.h, target, _p(gp0, C.c_float), _p(gp1, C.c_float),
+                                             _p(fl, C.c_uint8)))
+        return gp0, gp1, fl
 
     def stage_times(self):
         ms = np.zeros(5, np.float32)

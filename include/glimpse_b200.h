@@ -34,6 +34,13 @@ extern "C" {
 #define GP_E_STATE (-4)    /* call out of order (e.g. no targets set) */
 #define GP_E_DATA (-5)     /* inconsistent input data (e.g. zero states) */
 
+/* Largest batch per call: targets per context (gp_targets_set; each target
+ * has up to 2 haplotypes) and haplotypes or targets per call-level batch
+ * (gp_impute_batch, gp_rephase_batch). Batches index the second grid
+ * dimension of the kernel launches, whose hardware limit is 65535. */
+#define GP_MAX_TARGETS 32767
+#define GP_MAX_BATCH 65535
+
 #define GP_STAGE_INIT 0
 #define GP_STAGE_BURN 1
 #define GP_STAGE_MAIN 2
@@ -139,6 +146,13 @@ int gp_states_get(gp_ctx* ctx, int32_t target, uint32_t* states, int32_t* n_out)
 int gp_finalize(gp_ctx* ctx);
 int gp_gp_get(gp_ctx* ctx, float* gp0, float* gp1, float* ds, uint8_t* gt0, uint8_t* gt1);
 
+/* Parity hook: the genotype-posterior accumulators of one target as they
+ * stand (genotype::stored_data, genotype.h:38-78, before or after gp_finalize),
+ * dense over the L sites: gp0/gp1 the stored sums (normalised once finalised),
+ * flags bit 0 = an entry exists for the site (created when p0 / sum < 0.99999,
+ * genotype.cpp:127-209), bit 1 = hds. Sites without an entry read gp0 = gp1 = 0. */
+int gp_gp_accum_get(gp_ctx* ctx, int32_t target, float* gp0, float* gp1, uint8_t* flags);
+
 /* The record fields genotype_writer::writeGenotypes computes beyond GT and DS
  * (genotype_writer.cpp:110-190), after gp_finalize: gp (n x L x 3) the FORMAT/GP
  * values as written (floored to 1e-3, then raised by 1e-3 in the writer's order
@@ -178,10 +192,12 @@ int gp_impute_batch(gp_ctx* ctx, int32_t n, const int64_t* states_off, const uin
 /* No counterpart in the reference. The same computation as gp_impute_batch
  * with n = 1 (k sorted state ids; hl, hp: 2L floats; flat: L bytes), for
  * callers that must not allocate device memory during the call: all scratch
- * lives in one fixed 64 MiB region per device inside the library. Calls whose
- * scratch (about n_sites x k x 4 bytes, plus per-site records) would exceed it
- * return GP_E_ARG. The first call on a device looks the region up and should
- * come before any stream capture. Overlapping calls on one device race. */
+ * lives in one fixed 64 MiB region per device inside the library. The per-site
+ * buffers take about 51 x n_sites bytes plus n_sites / 32 x k x 4; the
+ * forward-backward store takes (polymorphic sites of the conditioning set) x
+ * k x 4 bytes from the rest. A call that does not fit returns GP_E_ARG before
+ * the HMM runs. The first call on a device looks the region up and should come
+ * before any stream capture. Overlapping calls on one device race. */
 int gp_impute_one_static(gp_ctx* ctx, int32_t k, const uint32_t* states, const float* hl, const uint8_t* flat,
                          float* hp);
 

@@ -43,3 +43,32 @@ def test_rephase_matches_reference(small_workload):
         if n0 or n1:
             bad.append((i, n0, n1, len(dip)))
     assert not bad, f"haplotype mismatches (case, #H0, #H1, nseg): {bad}"
+
+
+@pytest.mark.gpu
+def test_invalid_diplotype_sums_return_data_error(small_workload):
+    """SAMPLE_DIP with a NaN, infinite or sub-normal sum: the reference stops on
+    an assertion (phasing_hmm.cpp:175); the library finishes the call and
+    returns GP_E_DATA naming the target. A NaN err_phase makes every emission,
+    and so every diplotype sum, NaN. The oracle is not run here (it would abort
+    the process at that assertion)."""
+    from glimpse_b200 import native
+    w = small_workload
+    P, T = w.panel, w.targets
+    rng = np.random.default_rng(8)
+    good = native.Context(P)
+    bad = native.Context(P, err_phase=float("nan"))
+    try:
+        s = np.sort(rng.choice(P.n_ref_haps, size=64, replace=False)).astype(np.uint32)
+        h0 = _noisy_haps(rng, T.truth[1, 0])
+        h1 = _noisy_haps(rng, T.truth[1, 1])
+        good.rephase_batch([s], h0[None], h1[None], T.flat[1][None], 2, target_ids=[1])
+        with pytest.raises(native.GpError, match="target 7"):
+            bad.rephase_batch([s], h0[None], h1[None], T.flat[1][None], 2, target_ids=[7])
+        # the context stays usable: an iteration over the targets reports the same error
+        bad.set_targets(T, kpbwt=T.kpbwt)
+        with pytest.raises(native.GpError, match="invalid diplotype"):
+            bad.iteration(native.STAGE_INIT, 0)
+    finally:
+        good.close()
+        bad.close()

@@ -96,3 +96,45 @@ def test_pbwt_selection_haploid_target_matches_reference(pair_haploid):
         for lv, (r, g) in enumerate(zip(ref_lv, got_lv)):
             assert np.array_equal(r, g), f"target {t} level {lv}: {len(r)} vs {len(g)}"
         assert np.array_equal(orc.select(t, O.STAGE_BURN), ctx.states(t)), f"target {t} union differs"
+
+
+@pytest.mark.gpu
+def test_selection_with_capped_grid_matches_reference(small_workload, monkeypatch):
+    """The event-bit and panel-transpose kernels loop over their second grid
+    dimension when it would pass the hardware's 65,535 (panels with more than
+    about 2M events or common sites). GLIMPSE_B200_GRID_Y_CAP=2 makes a small
+    panel take those loops; selection must stay bit-exact and posteriors (which
+    read the transposed panel) within 1e-5 of the reference."""
+    O = ref_oracle_or_skip()
+    from glimpse_b200 import native
+    from conftest import init_hl
+    w = small_workload
+    T = w.targets
+    kw = dict(kinit=200, kpbwt=int(T.kpbwt.max()), pbwt_depth=8, pbwt_modulo_cm=0.05)
+    monkeypatch.setenv("GLIMPSE_B200_GRID_Y_CAP", "2")
+    ctx = native.Context(w.panel, **kw)
+    monkeypatch.delenv("GLIMPSE_B200_GRID_Y_CAP")
+    orc = O.RefOracle(w.panel, T, kpbwt_target=T.kpbwt, **kw)
+    try:
+        ctx.set_targets(T, kpbwt=T.kpbwt)
+        rng = np.random.default_rng(17)
+        h0 = np.stack([_noisy(rng, T.truth[t, 0], 0.02) for t in range(T.n)])
+        h1 = np.stack([_noisy(rng, T.truth[t, 1], 0.02) for t in range(T.n)])
+        for t in range(T.n):
+            orc.set_haps(t, h0[t], h1[t])
+        ctx.set_haps(h0, h1)
+        orc.pbwt_select(3, main_iteration=False)
+        ctx.select(O.STAGE_BURN, 3)
+        for t in range(T.n):
+            ref_lv = orc.pbwt_states(t)
+            got_lv = ctx.pbwt_states(t, depth=len(ref_lv))
+            for lv, (r, g) in enumerate(zip(ref_lv, got_lv)):
+                assert np.array_equal(r, g), f"target {t} level {lv}"
+            assert np.array_equal(orc.select(t, O.STAGE_BURN), ctx.states(t)), f"target {t} union differs"
+        s = ctx.states(0)
+        hl = init_hl(T.gl[0], T.flat[0])
+        got = ctx.impute_batch([s], hl[None], T.flat[0][None])[0]
+        ref, _ = orc.impute(s, hl, T.flat[0])
+        assert float(np.abs(got - ref).max()) <= 1e-5
+    finally:
+        ctx.close()
