@@ -236,6 +236,8 @@ Context::~Context() {
   glin_err.release();
   out_gp.release(); out_site.release();
   lig_a.release(); lig_b.release(); lig_s.release(); lig_cnt.release();
+  for (DevBuf* b : mlp.all()) b->release();
+  for (DevBuf* b : learned.all()) b->release();
   if (phase_err_host) cudaFreeHost(phase_err_host);
   if (stream) cudaStreamDestroy(stream);
 }

@@ -4,6 +4,8 @@
 #include <vector>
 
 #include "internal.h"
+#include "learned.h"
+#include "mlp.h"
 #include "select.h"
 
 namespace gp {
@@ -71,6 +73,8 @@ struct Context {
   std::vector<int32_t> phase_err_ids;  // target reported for each flag
   int check_phase_errors();
   TargetWork tw;
+  MlpState mlp;          // the learned proposal's network (mlp.cu)
+  LearnedWork learned;   // the learned proposal around it (learned.cu)
   SparsePbwt sparse;
   DevPbwt pbwt;
   bool pbwt_active = false;
@@ -107,6 +111,11 @@ struct Context {
   int pbwt_prepare_targets();
   int pbwt_select_states(int stage, int iteration, int Kp);
   int pbwt_states_get(int target, int32_t* counts, int32_t* states, int cap);
+  int learned_prepare_panel();
+  int learned_features(int Kpc, DevBuf& xout);
+  int learned_select_states(int stage, int iteration, int& Kp);
+  int learned_labels(int Kpc, float kpos, DevBuf& yout, DevBuf& wout);
+  int learned_apply_k();
   int run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_host, int nb, uint8_t* d_h0, uint8_t* d_h1,
                 const uint8_t* d_flat, int iteration, const int32_t* d_target_ids);
 };

@@ -66,9 +66,8 @@ int Context::set_targets(int n, const uint8_t* gl, const uint8_t* flat, const in
   T.stored_cnt = 0;
   T.finalized = false;
   if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(e, "targets upload");
-  int rc = pbwt_prepare_targets();
-  if (rc != GP_OK) return rc;
-  return GP_OK;
+  learned.kfinal.clear();  // the caller's Kpbwt becomes the learned mode's conditioning-set size
+  return learned_apply_k();
 }
 
 // Conditioning sets from states already on the device (impute.states with
@@ -156,6 +155,7 @@ int Context::select_states(int stage, int iteration, int& Kp) {
     prof.kernel_launches += 2;
     return GP_OK;
   }
+  if (learned.on && mlp.ready) return learned_select_states(stage, iteration, Kp);
   return pbwt_select_states(stage, iteration, Kp);
 }
 

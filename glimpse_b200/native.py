@@ -25,6 +25,8 @@ EXPORTS = [
     "gp_impute_one_static",
     "gp_targets_reset", "gp_gl_from_pl", "gp_gl_from_float", "gp_output_records", "gp_ligate_overlap",
     "gp_ligate_swap", "gp_gp_accum_get",
+    "gp_mlp_param_count", "gp_mlp_init", "gp_mlp_set_params", "gp_mlp_get_params", "gp_mlp_forward",
+    "gp_mlp_train_step", "gp_learned_enable", "gp_learned_train", "gp_learned_windows", "gp_state_posteriors",
 ]
 
 
@@ -324,6 +326,73 @@ class Context:
         self._check(self.lib.gp_gp_accum_get(self.h, target, _p(gp0, C.c_float), _p(gp1, C.c_float),
                                              _p(fl, C.c_uint8)))
         return gp0, gp1, fl
+
+    # ---- learned state-selection proposal: the scoring network ----
+    def mlp_init(self, seed=1):
+        self._check(self.lib.gp_mlp_init(self.h, C.c_uint64(seed)))
+
+    def mlp_params(self):
+        p = np.zeros(self.lib.gp_mlp_param_count(), np.float32)
+        self._check(self.lib.gp_mlp_get_params(self.h, _p(p, C.c_float)))
+        return p
+
+    def mlp_set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        self._check(self.lib.gp_mlp_set_params(self.h, _p(p, C.c_float)))
+
+    def mlp_forward(self, x, hidden=False):
+        """Scores of feature rows x (n, 48); with hidden=True also the BF16 hidden activations."""
+        x = np.ascontiguousarray(x, np.float32)
+        n = x.shape[0]
+        sc = np.zeros(n, np.float32)
+        h1 = np.zeros((n, 256), np.float32) if hidden else None
+        h2 = np.zeros((n, 256), np.float32) if hidden else None
+        self._check(self.lib.gp_mlp_forward(self.h, n, _p(x, C.c_float), _p(sc, C.c_float), _p(h1, C.c_float),
+                                            _p(h2, C.c_float)))
+        return (sc, h1, h2) if hidden else sc
+
+    def mlp_train_step(self, x, y, wt=None, lr=0.0, grad=False):
+        """One step; returns (loss, grad or None)."""
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        wt = None if wt is None else np.ascontiguousarray(wt, np.float32)
+        g = np.zeros(self.lib.gp_mlp_param_count(), np.float32) if grad else None
+        loss = C.c_float(0.0)
+        self._check(self.lib.gp_mlp_train_step(self.h, x.shape[0], _p(x, C.c_float), _p(y, C.c_float),
+                                               _p(wt, C.c_float), C.c_float(lr), C.byref(loss), _p(g, C.c_float)))
+        return loss.value, g
+
+    def learned_windows(self):
+        n = self.lib.gp_learned_windows(self.h)
+        if n < 0:
+            self._check(n)
+        return n
+
+    def state_posteriors(self, states_list, hl, flat):
+        """gp_state_posteriors: per haplotype an array (nwin, K_i) of window masses, and nsites (n, nwin)."""
+        n = len(states_list)
+        nwin = self.learned_windows()
+        off = np.zeros(n + 1, np.int64)
+        off[1:] = np.cumsum([len(s) for s in states_list])
+        st = np.ascontiguousarray(np.concatenate([np.asarray(s, np.uint32) for s in states_list]), np.uint32)
+        hl = np.ascontiguousarray(hl, np.float32).reshape(n, 2 * self.L)
+        flat = np.ascontiguousarray(flat, np.uint8).reshape(n, self.L)
+        mass = np.zeros(nwin * int(off[-1]), np.float32)
+        ns = np.zeros((n, nwin), np.int32)
+        self._check(self.lib.gp_state_posteriors(self.h, n, _p(off, C.c_int64), _p(st, C.c_uint32), _p(hl, C.c_float),
+                                                 _p(flat, C.c_uint8), _p(mass, C.c_float), _p(ns, C.c_int32)))
+        out = [mass[nwin * off[i]:nwin * off[i + 1]].reshape(nwin, len(states_list[i])) for i in range(n)]
+        return out, ns
+
+    def learned_enable(self, enable=True, kcand=1024):
+        self._check(self.lib.gp_learned_enable(self.h, int(enable), kcand))
+
+    def learned_train(self, kcand=1024, kpos=8.0, steps=300, batch=16384, lr=1e-3, seed=1):
+        """gp_learned_train on the current targets; returns the per-step losses."""
+        losses = np.zeros(max(steps, 1), np.float32)
+        self._check(self.lib.gp_learned_train(self.h, kcand, C.c_float(kpos), steps, batch, C.c_float(lr),
+                                              C.c_uint64(seed), _p(losses, C.c_float)))
+        return losses[:steps]
 
     def stage_times(self):
         ms = np.zeros(5, np.float32)

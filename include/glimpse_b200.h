@@ -228,6 +228,71 @@ int gp_sparse_pbwt_get(gp_ctx* ctx, uint8_t* ypacked, int64_t* ypacked_len, int6
 int gp_build_sparse_pbwt(const gp_panel_desc* panel, uint8_t* ypacked, int64_t* ypacked_len, int64_t* asmall_off,
                          int32_t* asmall_idx, int64_t* asmall_len);
 
+/* ---- Learned state-selection proposal: the scoring network ----
+ * No counterpart in the reference, which selects conditioning states by PBWT
+ * alone (haplotype_set.cpp:682-728, conditioning_set.cpp:96-104). An MLP
+ * scores candidate reference haplotypes from 48 features per candidate:
+ * 48 -> 256 -> 256 -> 1 with ReLU, BF16 weights and activations, FP32
+ * accumulation, forward and backward on the tensor cores. Parameters are one
+ * packed FP32 vector of gp_mlp_param_count() values: W1 [256][64] (row = hidden
+ * unit; columns 48..63 are padding and must be zero), b1 [256], W2 [256][256]
+ * (row = output unit), b2 [256], w3 [256], b3 [1]. */
+int32_t gp_mlp_param_count(void);
+/* He-uniform weights from a seed, zero biases; resets the optimiser. */
+int gp_mlp_init(gp_ctx* ctx, uint64_t seed);
+int gp_mlp_set_params(gp_ctx* ctx, const float* params);
+int gp_mlp_get_params(gp_ctx* ctx, float* params);
+/* Scores of n feature rows x (n x 48 FP32, rounded to BF16 on the device);
+ * h1, h2 (n x 256, optional) receive the BF16 hidden activations. */
+int gp_mlp_forward(gp_ctx* ctx, int32_t n, const float* x, float* score, float* h1, float* h2);
+/* One training step on n rows: loss = sum_i wt_i BCE(sigmoid(score_i), y_i) / n
+ * (wt NULL: 1), gradients by the backward kernels, then one Adam step with
+ * learning rate lr (lr = 0: no update). loss and grad (gp_mlp_param_count()
+ * values, before the update) are optional outputs. */
+int gp_mlp_train_step(gp_ctx* ctx, int32_t n, const float* x, const float* y, const float* wt, float lr, float* loss,
+                      float* grad);
+
+/* ---- Learned state-selection proposal ----
+ * No counterpart in the reference. With it enabled, burn-in and main
+ * iterations select each target's conditioning states in place of the union of
+ * conditioning_set::compactSelection (conditioning_set.cpp:96-104): the PBWT
+ * selection (haplotype_set.cpp:317-728) runs with kcand states per target to
+ * give candidates; every (target, window of 256 common sites, candidate) gets
+ * 48 features (matches with the target's two current haplotypes over the
+ * window and its neighbours, match runs through the window, agreement with
+ * confident genotype-likelihood calls, densities); the network scores them;
+ * per window the top 32 candidates are ranked, and the conditioning set is the
+ * union in rank order cut at the target's Kpbwt (gp_targets_set). The init
+ * stage is unchanged. Disabled (the default), selection is the plain PBWT path.
+ * Enabling needs network parameters (gp_mlp_init, gp_mlp_set_params or
+ * gp_learned_train); kcand is at most 2048. */
+int gp_learned_enable(gp_ctx* ctx, int32_t enable, int32_t kcand);
+
+/* Windows of the learned proposal: runs of 256 consecutive common sites; a
+ * rare site belongs to the window of the last common site before it. */
+int32_t gp_learned_windows(gp_ctx* ctx);
+
+/* Per-window state posteriors (the learned proposal's training labels) for n
+ * haplotypes with explicit conditioning sets, as gp_impute_batch takes them:
+ * the HMM of imputation_hmm (imputation_hmm.cpp:80-353) over the set, with
+ * per-site normalisation; for haplotype i, window w and state j of its set,
+ * mass[nwin * states_off[i] + w * K_i + j] = sum over the window's polymorphic
+ * sites of alpha(j) beta(j) / sum_j' alpha(j') beta(j'); nsites (n x nwin)
+ * counts those sites. nwin = gp_learned_windows(ctx). */
+int gp_state_posteriors(gp_ctx* ctx, int32_t n, const int64_t* states_off, const uint32_t* states, const float* hl,
+                        const uint8_t* flat, float* mass, int32_t* nsites);
+
+/* Train the network on the context's current targets and haplotypes (run a few
+ * plain iterations first): candidates from the PBWT selection at kcand; labels
+ * from the HMM over all candidates of each target, per window the larger of the
+ * two haplotypes' posterior share q of a candidate, y = min(1, kpos q), weight
+ * 1 + 10 y; then `steps` Adam steps (learning rate lr) on batches of `batch`
+ * rows (a multiple of 128) drawn without replacement, reshuffled each pass.
+ * losses (optional, steps values) receives each step's loss. Initialises the
+ * network from seed when it has no parameters. */
+int gp_learned_train(gp_ctx* ctx, int32_t kcand, float kpos, int32_t steps, int32_t batch, float lr, uint64_t seed,
+                     float* losses);
+
 /* Timing of the last gp_iteration by stage, in milliseconds (device events). */
 int gp_stage_times(gp_ctx* ctx, float* ms, int32_t n);
 

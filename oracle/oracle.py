@@ -317,6 +317,12 @@ def restate_lib():
                                   C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_uint32), C.c_int,
                                   C.c_double, C.c_float, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_uint8),
                                   C.POINTER(C.c_float)]
+        lib.rs_state_post.restype = None
+        lib.rs_state_post.argtypes = [C.c_int, C.POINTER(C.c_uint8), C.POINTER(C.c_uint8), C.POINTER(C.c_uint8),
+                                      C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_uint8), C.c_int,
+                                      C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_uint32), C.c_int,
+                                      C.c_double, C.c_float, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_uint8),
+                                      C.POINTER(C.c_int32), C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int32)]
         _restate = lib
     return _restate
 
@@ -345,3 +351,40 @@ def restate_impute(panel, states, HL, flat, precision=64, ne=100000, err_imp=1e-
                        _p(keep[8], C.c_uint32), keep[8].size, nrho, float(ed), float(ee), _p(keep[9], C.c_float),
                        _p(keep[10], C.c_uint8), _p(HP, C.c_float))
     return HP, ll
+
+
+def panel_windows(panel, win_sites=256):
+    """Window of every panel site for the learned proposal: that of the last
+    common site at or before it, windows of win_sites common sites."""
+    com = np.asarray(panel.flag_common, bool)
+    r = np.cumsum(com) - 1
+    return (np.maximum(r, 0) // win_sites).astype(np.int32), max(1, (int(com.sum()) + win_sites - 1) // win_sites)
+
+
+def restate_state_post(panel, states, HL, flat, ne=100000, err_imp=1e-12):
+    """FP64 per-window state posteriors (mass (nwin, K), nsites (nwin,))."""
+    lib = restate_lib()
+    L = panel.n_sites
+    comrow = np.full(L, -1, np.int32)
+    com = np.flatnonzero(panel.flag_common)
+    comrow[com] = np.arange(com.size, dtype=np.int32)
+    sw, nwin = panel_windows(panel)
+    keep = [np.ascontiguousarray(x) for x in (panel.flag_common.astype(np.uint8), panel.lq.astype(np.uint8),
+                                              panel.major.astype(np.uint8), panel.cm.astype(np.float64), comrow,
+                                              panel.hvar.astype(np.uint8), panel.shap_off.astype(np.int64),
+                                              panel.shap_sites.astype(np.int32),
+                                              np.asarray(states, np.uint32), np.asarray(HL, np.float32),
+                                              np.asarray(flat, np.uint8), sw)]
+    K = keep[8].size
+    mass = np.zeros(nwin * K, np.float64)
+    ns = np.zeros(nwin, np.int32)
+    err = float(np.clip(np.float32(err_imp), np.float32(1e-12), np.float32(1e-3)))
+    ed = np.float32(err)
+    ee = np.float32(1.0 - float(ed))
+    lib.rs_state_post(L, _p(keep[0], C.c_uint8), _p(keep[1], C.c_uint8), _p(keep[2], C.c_uint8),
+                      _p(keep[3], C.c_double), _p(keep[4], C.c_int32), _p(keep[5], C.c_uint8),
+                      (panel.n_ref_haps + 7) // 8, _p(keep[6], C.c_int64), _p(keep[7], C.c_int32),
+                      _p(keep[8], C.c_uint32), K, (-0.04 * ne) / panel.n_ref_haps, float(ed), float(ee),
+                      _p(keep[9], C.c_float), _p(keep[10], C.c_uint8), _p(keep[11], C.c_int32), nwin,
+                      _p(mass, C.c_double), _p(ns, C.c_int32))
+    return mass.reshape(nwin, K), ns

@@ -169,3 +169,90 @@ double rs_impute(int precision, int L, const uint8_t* common, const uint8_t* lq,
   return impute_f32(L, common, lq, major, cm, comrow, hvar, stride, shap_off, shap_sites, states, K, nrho, ed, ee, HL,
                     flat, HP);
 }
+
+/* Per-window state posteriors, FP64: the label HMM of the learned state
+ * selection (no counterpart in the reference). For the conditioning set built
+ * as above, mass[w * K + k] = sum over the polymorphic sites l with
+ * site_win[l] == w of alpha_l(k) beta_l(k) / sum_k' alpha_l(k') beta_l(k'),
+ * alpha_l including the emission at l and beta_l the backward message
+ * without it (beta = 1 at the last site); nsites[w] counts those sites. */
+void rs_state_post(int L, const uint8_t* common, const uint8_t* lq, const uint8_t* major, const double* cm,
+                   const int32_t* comrow, const uint8_t* hvar, int stride, const int64_t* shap_off,
+                   const int32_t* shap_sites, const uint32_t* states, int K, double nrho, float ed_f, float ee_f,
+                   const float* HL, const uint8_t* flat, const int32_t* site_win, int nwin, double* mass,
+                   int32_t* nsites) {
+  const double ed = ed_f, ee = ee_f;
+  uint8_t* poly = (uint8_t*)calloc(L, 1);
+  int32_t* plist = (int32_t*)malloc(sizeof(int32_t) * L);
+  int np = 0;
+  for (int l = 0; l < L; ++l) poly[l] = common[l];
+  for (int k = 0; k < K; ++k)
+    for (int64_t j = shap_off[states[k]]; j < shap_off[states[k] + 1]; ++j) poly[shap_sites[j]] = 1;
+  for (int l = 0; l < L; ++l)
+    if (poly[l]) plist[np++] = l;
+  uint8_t* bits = (uint8_t*)malloc((size_t)np * K + 1);
+  int32_t* lrel = (int32_t*)malloc(sizeof(int32_t) * L);
+  for (int i = 0; i < np; ++i) lrel[plist[i]] = i;
+  for (int i = 0; i < np; ++i) {
+    const int s = plist[i];
+    for (int k = 0; k < K; ++k) {
+      const int h = (int)states[k];
+      bits[(size_t)i * K + k] =
+          common[s] ? (hvar[(size_t)comrow[s] * stride + (h >> 3)] >> (7 - (h & 7))) & 1 : major[s];
+    }
+  }
+  for (int k = 0; k < K; ++k)
+    for (int64_t j = shap_off[states[k]]; j < shap_off[states[k] + 1]; ++j)
+      bits[(size_t)lrel[shap_sites[j]] * K + k] = !major[shap_sites[j]];
+  double* t = (double*)malloc(sizeof(double) * (np + 1));
+  for (int i = 1; i < np; ++i) {
+    double x = -expm1(nrho * (cm[plist[i]] - cm[plist[i - 1]]));
+    x = x < 1e-7 ? 1e-7 : (x > 1.0 - 1e-7 ? 1.0 - 1e-7 : x);
+    t[i - 1] = (double)(float)x;
+  }
+  double* alpha = (double*)malloc(sizeof(double) * (size_t)np * K + 8);
+  double* beta = (double*)malloc(sizeof(double) * (K + 1));
+  double* nb = (double*)malloc(sizeof(double) * (K + 1));
+  double* em = (double*)malloc(sizeof(double) * 2 * (np + 1));
+  for (int i = 0; i < np; ++i) {
+    const int s = plist[i];
+    if (flat[s] || lq[s]) {
+      em[2 * i] = em[2 * i + 1] = 1.0;
+    } else {
+      const double p0 = (double)HL[2 * s] * ee + (double)HL[2 * s + 1] * ed;
+      const double p1 = (double)HL[2 * s] * ed + (double)HL[2 * s + 1] * ee;
+      em[2 * i] = p0 / (p0 + p1);
+      em[2 * i + 1] = p1 / (p0 + p1);
+    }
+  }
+  for (int i = 0; i < np; ++i) {
+    double* a = alpha + (size_t)i * K;
+    double sum = 0;
+    for (int k = 0; k < K; ++k) {
+      const double prev = i == 0 ? 1.0 / K : alpha[(size_t)(i - 1) * K + k] * (1.0 - t[i - 1]) + t[i - 1] / K;
+      a[k] = prev * em[2 * i + bits[(size_t)i * K + k]];
+      sum += a[k];
+    }
+    for (int k = 0; k < K; ++k) a[k] /= sum;
+  }
+  for (int w = 0; w < nwin; ++w) nsites[w] = 0;
+  for (size_t j = 0; j < (size_t)nwin * K; ++j) mass[j] = 0.0;
+  for (int k = 0; k < K; ++k) beta[k] = 1.0;
+  for (int i = np - 1; i >= 0; --i) {
+    if (i < np - 1) {
+      double se = 0;
+      for (int k = 0; k < K; ++k) {
+        nb[k] = em[2 * (i + 1) + bits[(size_t)(i + 1) * K + k]] * beta[k];
+        se += nb[k];
+      }
+      for (int k = 0; k < K; ++k) beta[k] = nb[k] / se * (1.0 - t[i]) + t[i] / K;
+    }
+    const double* a = alpha + (size_t)i * K;
+    double z = 0;
+    for (int k = 0; k < K; ++k) z += a[k] * beta[k];
+    const int w = site_win[plist[i]];
+    nsites[w]++;
+    for (int k = 0; k < K; ++k) mass[(size_t)w * K + k] += a[k] * beta[k] / z;
+  }
+  free(poly); free(plist); free(bits); free(lrel); free(t); free(alpha); free(beta); free(nb); free(em);
+}

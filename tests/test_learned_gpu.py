@@ -1,0 +1,98 @@
+"""The learned state-selection proposal through the C-ABI.
+
+  * Label HMM: per-window state posteriors (gp_state_posteriors) against the
+    FP64 restatement (oracle/restate.c rs_state_post) on identical inputs.
+  * The proposal runs inside a Gibbs iteration: trained on the targets' own
+    HMM posteriors, enabled for a burn-in iteration, it yields sorted, unique
+    conditioning sets of at most each target's K drawn from the PBWT
+    candidates, and posteriors that are probabilities.
+  * Plain PBWT selection is restored when the proposal is disabled: the
+    iteration matches a context that never enabled it."""
+import numpy as np
+import pytest
+
+from conftest import init_hl
+
+
+@pytest.mark.gpu
+def test_state_posteriors_match_fp64(small_workload):
+    from glimpse_b200 import native
+    from oracle import oracle as O
+    w = small_workload
+    P, T = w.panel, w.targets
+    ctx = native.Context(P)
+    try:
+        rng = np.random.default_rng(4)
+        states, hls, flats = [], [], []
+        for t, K in zip(range(T.n), (37, 256, 599)):
+            states.append(np.sort(rng.choice(P.n_ref_haps, K, replace=False)).astype(np.uint32))
+            hls.append(init_hl(T.gl[t], T.flat[t]))
+            flats.append(T.flat[t])
+        mass, ns = ctx.state_posteriors(states, np.stack(hls), np.stack(flats))
+        for i in range(len(states)):
+            ref, rns = O.restate_state_post(P, states[i], hls[i], flats[i])
+            assert np.array_equal(ns[i], rns)
+            # each polymorphic site contributes posteriors that sum to 1
+            assert np.allclose(mass[i].sum(1), ns[i], rtol=1e-4, atol=1e-3)
+            err = float(np.abs(mass[i] - ref).max())
+            assert err <= 2e-4 * max(1, int(ns[i].max())) ** 0.5, f"haplotype {i}: max |dmass| {err:.2e}"
+    finally:
+        ctx.close()
+
+
+def _workload():
+    from glimpse_b200 import synth
+    return synth.make_panel_and_targets(2000, 12000, 1.5, 0.6, 8, ("uniform", 0.5, 2.0), ("fixed", 120), seed=31,
+                                        sparse_maf=0.005)
+
+
+@pytest.mark.gpu
+def test_learned_selection_in_iteration():
+    from glimpse_b200 import native
+    w = _workload()
+    P, T = w.panel, w.targets
+    kw = dict(kinit=300, kpbwt=120, pbwt_depth=8, pbwt_modulo_cm=0.05)
+    ctx = native.Context(P, **kw)
+    try:
+        ctx.set_targets(T, kpbwt=T.kpbwt)
+        ctx.iteration(native.STAGE_INIT, 0)
+        ctx.iteration(native.STAGE_BURN, 1)
+        losses = ctx.learned_train(kcand=512, kpos=8.0, steps=60, batch=4096, lr=1e-3, seed=2)
+        assert np.isfinite(losses).all()
+        assert losses[-10:].mean() < losses[:10].mean()
+        ctx.learned_enable(True, kcand=512)
+        ctx.iteration(native.STAGE_BURN, 2)
+        for t in range(T.n):
+            st = ctx.states(t)
+            assert 0 < st.size <= T.kpbwt[t]
+            assert np.all(np.diff(st.astype(np.int64)) > 0)
+            h0, h1 = ctx.posteriors(t)
+            assert np.isfinite(h0).all() and np.isfinite(h1).all()
+            assert np.allclose(h0[0::2] + h0[1::2], 1.0, atol=1e-4)
+    finally:
+        ctx.close()
+
+
+@pytest.mark.gpu
+def test_disabling_restores_plain_selection():
+    from glimpse_b200 import native
+    w = _workload()
+    P, T = w.panel, w.targets
+    kw = dict(kinit=300, kpbwt=120, pbwt_depth=8, pbwt_modulo_cm=0.05)
+    a, b = native.Context(P, **kw), native.Context(P, **kw)
+    try:
+        for c in (a, b):
+            c.set_targets(T, kpbwt=T.kpbwt)
+            c.iteration(native.STAGE_INIT, 0)
+        a.mlp_init(5)
+        a.learned_enable(True, kcand=400)
+        a.learned_enable(False, kcand=400)
+        a.iteration(native.STAGE_BURN, 1)
+        b.iteration(native.STAGE_BURN, 1)
+        for t in range(T.n):
+            assert np.array_equal(a.states(t), b.states(t))
+        ha, hb = a.haps(), b.haps()
+        assert np.array_equal(ha[0], hb[0]) and np.array_equal(ha[1], hb[1])
+    finally:
+        a.close()
+        b.close()
