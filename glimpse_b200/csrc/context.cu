@@ -290,7 +290,26 @@ int Context::build_condsets(int n, const std::vector<int64_t>& off, const std::v
   return GP_OK;
 }
 
-// Forward-backward over the current conditioning sets.
+// Bytes the forward-backward store may take: half of the device's memory, and
+// no more than is free now (plus what the store already holds) less 8 GiB for
+// the rest of the iteration. GLIMPSE_B200_STORE_BUDGET_MB lowers it (tests use
+// it to run the chunked path on small batches).
+size_t Context::store_budget(size_t held) {
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return held;
+  const size_t reserve = size_t(8) << 30;
+  size_t b = std::min(tot / 2, fr + held > reserve ? fr + held - reserve : held);
+  if (const char* env = std::getenv("GLIMPSE_B200_STORE_BUDGET_MB")) {
+    const long long mb = std::atoll(env);
+    if (mb > 0) b = std::min(b, (size_t)mb << 20);
+  }
+  return b;
+}
+
+// Forward-backward over the current conditioning sets. The haplotypes run in
+// decreasing order of polymorphic sites; when their stores do not fit the
+// budget together, they run in consecutive chunks of that order, each chunk's
+// stores packed from the start of the buffer.
 int Context::run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
   ImputeWork& w = impute;
   const int n = w.n, L = w.L;
@@ -299,29 +318,38 @@ int Context::run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
   if ((e = w.tr.ensure((size_t)n * L * 8)) != cudaSuccess) return cuda_fail(e, "alloc tr");
   if ((e = w.fl.ensure((size_t)n * L)) != cudaSuccess) return cuda_fail(e, "alloc fl");
   if ((e = w.alpha_off.ensure((size_t)n * 8)) != cudaSuccess) return cuda_fail(e, "alloc alpha_off");
+  int Kmax = 0;
+  for (int i = 0; i < n; ++i) Kmax = std::max(Kmax, host_nstates[i]);
+  w.Ks = impute_store_stride(Kmax);
+  // Chains of the longest haplotypes (most poly sites) are launched first.
+  std::vector<int32_t> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return impute_np[x] > impute_np[y]; });
+  // chunks of the order whose stores fit the budget
+  const size_t budget = store_budget(w.alpha.cap);
   std::vector<int64_t> aoff(n);
   std::vector<int32_t> split(n);
-  int64_t tot = 0;
-  int Kmax = 0;
-  int Kall = 0;
-  for (int i = 0; i < n; ++i) Kall = std::max(Kall, host_nstates[i]);
-  w.Ks = impute_store_stride(Kall);
-  for (int i = 0; i < n; ++i) {
-    aoff[i] = tot;
-    tot += (int64_t)impute_np[i] * w.Ks;
+  std::vector<int> chunk_start(1, 0);
+  int64_t tot = 0, need = 0;
+  for (int j = 0; j < n; ++j) {
+    const int i = order[j];
+    const int64_t bytes = (int64_t)impute_np[i] * w.Ks * 4;
+    if (j > chunk_start.back() && (size_t)(tot + bytes) > budget) {
+      chunk_start.push_back(j);
+      tot = 0;
+    }
+    aoff[i] = tot / 4;
+    tot += bytes;
+    need = std::max(need, tot);
     split[i] = (impute_np[i] / 2) & ~31;  // forward/backward meeting point, a multiple of 32
-    Kmax = std::max(Kmax, host_nstates[i]);
   }
-  if ((e = w.alpha.ensure((size_t)std::max<int64_t>(tot, 1) * 4)) != cudaSuccess) return cuda_fail(e, "alloc alpha");
+  chunk_start.push_back(n);
+  if ((e = w.alpha.ensure((size_t)std::max<int64_t>(need, 4))) != cudaSuccess) return cuda_fail(e, "alloc alpha");
   if ((e = w.split.ensure((size_t)n * 4)) != cudaSuccess) return cuda_fail(e, "alloc split");
   if ((e = w.split_scr.ensure(((size_t)((2 * n + 3) & ~3) + (size_t)n * w.Ks) * 4)) != cudaSuccess)
     return cuda_fail(e, "alloc split");
   cudaMemcpyAsync(w.alpha_off.ptr, aoff.data(), n * 8, cudaMemcpyHostToDevice, stream);
   cudaMemcpyAsync(w.split.ptr, split.data(), n * 4, cudaMemcpyHostToDevice, stream);
-  // Chains of the longest haplotypes (most poly sites) are launched first.
-  std::vector<int32_t> order(n);
-  for (int i = 0; i < n; ++i) order[i] = i;
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return impute_np[x] > impute_np[y]; });
   if ((e = w.order.ensure((size_t)n * 4)) != cudaSuccess) return cuda_fail(e, "alloc order");
   cudaMemcpyAsync(w.order.ptr, order.data(), (size_t)n * 4, cudaMemcpyHostToDevice, stream);
   launch_site_records(panel, mc, w, d_hl, d_flat, stream);
@@ -331,13 +359,18 @@ int Context::run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
   const int J = impute_groups(Kmax);
   cudaEvent_t ea;
   prof_begin(ea);
-  int lrc = launch_impute_warp(1, J, mc, w, d_hp, stream);
-  if (lrc == GP_OK) lrc = launch_impute_warp(2, J, mc, w, d_hp, stream);
-  if (lrc == GP_E_CUDA) return cuda_fail(cudaGetLastError(), "imputation: shared-memory attribute");
-  if (lrc != GP_OK) return (fail(GP_E_ARG, "imputation: too many states"), GP_E_ARG);
+  for (size_t c = 0; c + 1 < chunk_start.size(); ++c) {
+    const int j0 = chunk_start[c], nc = chunk_start[c + 1] - j0;
+    int lrc = launch_impute_warp(1, J, mc, w, d_hp, stream, j0, nc);
+    if (lrc == GP_OK) lrc = launch_impute_warp(2, J, mc, w, d_hp, stream, j0, nc);
+    if (lrc == GP_E_CUDA) return cuda_fail(cudaGetLastError(), "imputation: shared-memory attribute");
+    if (lrc != GP_OK) return (fail(GP_E_ARG, "imputation: too many states"), GP_E_ARG);
+    prof.kernel_launches += 2;
+  }
   prof_end(ea, 0, cells);
+  impute_chunks = (int)chunk_start.size() - 1;
   launch_impute_finish(panel, mc, w, d_hl, d_flat, d_hp, stream);
-  prof.kernel_launches += 4;
+  prof.kernel_launches += 2;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "imputation launch");
   return GP_OK;
 }

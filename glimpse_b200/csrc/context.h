@@ -102,6 +102,8 @@ struct Context {
   int create_panel(const gp_panel_desc& d);
   int build_condsets(int n, const std::vector<int64_t>& off, const std::vector<uint32_t>& states);
   int run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp);
+  size_t store_budget(size_t held);
+  int impute_chunks = 0;  // launches pairs of the last run_impute (1 when the whole batch fit)
   int set_targets(int n, const uint8_t* gl, const uint8_t* flat, const int32_t* ploidy, const int32_t* kp);
   int build_condsets_device(int n, int Kp);
   int select_states(int stage, int iteration, int& Kp);

@@ -515,13 +515,17 @@ static int launch_chains(const ChainArgs& a, cudaStream_t s) {
   return GP_OK;
 }
 
-int launch_impute_warp(int phase, int J, const ModelConst& mc, ImputeWork& w, float* hp, cudaStream_t s) {
+int launch_impute_warp(int phase, int J, const ModelConst& mc, ImputeWork& w, float* hp, cudaStream_t s, int first,
+                       int count) {
   ChainArgs a;
   a.sc.asum = w.split_scr.as<float>();
   a.sc.bsum = a.sc.asum + w.n;
   a.sc.brow = a.sc.asum + ((2 * w.n + 3) & ~3);  // 16-byte aligned rows of Ks floats
   a.sc.split = w.split.as<int32_t>();
-  a.nchains = 2 * w.n;
+  if (count < 0) count = w.n;
+  if (first < 0 || first + count > w.n || (first > 0 && !w.order.ptr)) return GP_E_ARG;
+  if (count == 0) return GP_OK;
+  a.nchains = 2 * count;
   a.poly = w.poly.as<int32_t>();
   a.npoly = w.npoly.as<int32_t>();
   a.nstates = w.nstates.as<int32_t>();
@@ -537,7 +541,7 @@ int launch_impute_warp(int phase, int J, const ModelConst& mc, ImputeWork& w, fl
   a.Ks = w.Ks;
   a.mc = mc;
   a.hp = hp;
-  a.order = w.order.as<int32_t>();
+  a.order = w.order.ptr ? w.order.as<int32_t>() + first : nullptr;
 #define GP_WARP(JJ) \
   case JJ: return phase == 2 ? launch_chains<JJ, true>(a, s) : launch_chains<JJ, false>(a, s);
   switch (J) {

@@ -33,3 +33,31 @@ def test_impute_matches_reference(small_workload):
     for i, r in enumerate(refs):
         err = np.abs(hp[i] - r).max()
         assert err <= TOL, f"case {i}: max |dHP| = {err}"
+
+
+@pytest.mark.gpu
+def test_chunked_store_matches_single_launch(small_workload, monkeypatch):
+    """When the haplotypes' forward-backward stores do not fit the device-memory
+    budget together, they run in consecutive chunks (GLIMPSE_B200_STORE_BUDGET_MB
+    lowers the budget so that a small batch takes that path). The posteriors
+    must be identical to the single-launch run."""
+    from glimpse_b200 import native
+    from conftest import init_hl
+    w = small_workload
+    P, T = w.panel, w.targets
+    rng = np.random.default_rng(12)
+    states, hls, flats = [], [], []
+    for i in range(9):
+        t = i % T.n
+        states.append(np.sort(rng.choice(P.n_ref_haps, int(rng.integers(40, 500)), replace=False)).astype(np.uint32))
+        hls.append(init_hl(T.gl[t], T.flat[t]))
+        flats.append(T.flat[t])
+    ctx = native.Context(P)
+    try:
+        whole = ctx.impute_batch(states, np.stack(hls), np.stack(flats))
+        monkeypatch.setenv("GLIMPSE_B200_STORE_BUDGET_MB", "4")
+        chunked = ctx.impute_batch(states, np.stack(hls), np.stack(flats))
+        monkeypatch.delenv("GLIMPSE_B200_STORE_BUDGET_MB")
+        assert np.array_equal(whole, chunked)
+    finally:
+        ctx.close()
