@@ -381,6 +381,80 @@ def run_ours(args):
     return 0
 
 
+def run_learned(args):
+    """Learned proposal against plain PBWT selection on one GPU, device-timed
+    complete runs (1 init + 5 burn-in + 15 main, finalisation) of the workload's
+    benchmark targets. The network is trained first on a separate set of
+    simulated targets of the same panel (their own plain init and burn-in
+    iterations give the haplotypes; labels are the HMM's window posteriors over
+    their PBWT candidates). Reported: samples/s and dosage r2 of plain selection
+    at the workload's K, plain at K x --learned-frac, and the learned proposal at
+    K x --learned-frac (candidates: PBWT at the workload's K)."""
+    import torch
+    from glimpse_b200 import native
+    torch.cuda.set_device(0)
+    n_test = synth.CONFIGS[args.config]["n_targets"]
+    w = synth.workload(args.config, seed=1, n_targets=n_test + args.train_targets)
+    test = subset(w.targets, n_test)
+    import types
+    idx = np.arange(n_test, w.targets.n)
+    T = w.targets
+    train = types.SimpleNamespace(n=len(idx), ploidy=T.ploidy[idx], gl=T.gl[idx], flat=T.flat[idx],
+                                  truth=T.truth[idx], kpbwt=T.kpbwt[idx], coverage=T.coverage[idx])
+    kbig = test.kpbwt.copy()
+    ksmall = np.maximum(16, np.round(kbig * args.learned_frac)).astype(np.int32)
+    kcand = int(min(2048, kbig.max()))
+    ctx = native.Context(w.panel, kinit=w.params["kinit"], kpbwt=kcand, seed=15052011)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    t0 = time.perf_counter()
+    ctx.set_targets(train, kpbwt=np.full(train.n, kcand, np.int32))
+    ctx.iteration(native.STAGE_INIT, 0)
+    for it in range(1, 3):
+        ctx.iteration(native.STAGE_BURN, it)
+    losses = ctx.learned_train(kcand=kcand, kpos=8.0, steps=args.train_steps, batch=16384, lr=1e-3, seed=7)
+    t_train = time.perf_counter() - t0
+
+    def timed_runs(kp, learned):
+        ctx.learned_enable(False, kcand=kcand)
+        ctx.set_targets(test, kpbwt=kp)
+        if learned:
+            ctx.learned_enable(True, kcand=kcand)
+        for _ in range(args.warmup):
+            ctx.targets_reset()
+            ctx.run(BURNIN, MAIN)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            ctx.targets_reset()
+            ctx.run(BURNIN, MAIN)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        _, _, ds, _, _ = ctx.gp()
+        return {"samples_per_s": test.n / (ms / 1000.0), "ms_per_run": ms,
+                "dosage_r2": synth.dosage_r2(ds, test.truth.sum(1)), "k_mean": float(np.mean(kp))}
+
+    plain_big = timed_runs(kbig, False)
+    plain_small = timed_runs(ksmall, False)
+    learned_small = timed_runs(ksmall, True)
+    ctx.close()
+    matched = abs(learned_small["dosage_r2"] - plain_big["dosage_r2"]) <= 0.002
+    line = {"metric": "samples/s at matched dosage r2 (learned + batched vs plain)", "unit": "samples/s",
+            "value": learned_small["samples_per_s"], "higher_is_better": True, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "dtype": "f32 HMM, bf16 network", "data": "synthetic",
+            "config": {"workload": args.config, "targets": test.n, "training_targets": train.n,
+                       "training_steps": args.train_steps, "candidates_per_target": kcand,
+                       "k_fraction": args.learned_frac},
+            "plain_workload_k": plain_big, "plain_small_k": plain_small, "learned_small_k": learned_small,
+            "matched_r2": matched, "speedup_vs_plain": learned_small["samples_per_s"] / plain_big["samples_per_s"],
+            "r2_gain_vs_plain_same_k": learned_small["dosage_r2"] - plain_small["dosage_r2"],
+            "training": {"seconds": t_train, "loss_first": float(losses[:10].mean()),
+                         "loss_last": float(losses[-10:].mean())}}
+    print(json.dumps(line))
+    return 0
+
+
 def run_case(args):
     """Small cases of single stages, for profiler captures and quick timings
     (not bench lines): `iterations` runs Gibbs iterations of a workload with a
@@ -450,9 +524,16 @@ def main():
     ap.add_argument("--iterations", type=int, default=2)
     ap.add_argument("--fmt", choices=["PL", "GL"], default="PL")
     ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--learned", action="store_true",
+                    help="learned proposal vs plain PBWT selection (separate line; see run_learned)")
+    ap.add_argument("--learned-frac", type=float, default=0.4)
+    ap.add_argument("--train-targets", type=int, default=64)
+    ap.add_argument("--train-steps", type=int, default=400)
     args = ap.parse_args()
     if args.case:
         return run_case(args)
+    if args.learned:
+        return run_learned(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

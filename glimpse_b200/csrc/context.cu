@@ -237,6 +237,7 @@ Context::~Context() {
   out_gp.release(); out_site.release();
   lig_a.release(); lig_b.release(); lig_s.release(); lig_cnt.release();
   for (DevBuf* b : mlp.all()) b->release();
+  ckpt.release(); ckpt_sum.release(); ckpt_scratch.release(); loglik.release();
   for (DevBuf* b : learned.all()) b->release();
   if (phase_err_host) cudaFreeHost(phase_err_host);
   if (stream) cudaStreamDestroy(stream);
@@ -317,6 +318,7 @@ int Context::run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
   if ((e = w.em.ensure((size_t)n * L * 16)) != cudaSuccess) return cuda_fail(e, "alloc em");
   if ((e = w.tr.ensure((size_t)n * L * 8)) != cudaSuccess) return cuda_fail(e, "alloc tr");
   if ((e = w.fl.ensure((size_t)n * L)) != cudaSuccess) return cuda_fail(e, "alloc fl");
+  if (precision_mode != GP_PRECISION_FULL) return run_impute_ckpt(d_hl, d_flat, d_hp);
   if ((e = w.alpha_off.ensure((size_t)n * 8)) != cudaSuccess) return cuda_fail(e, "alloc alpha_off");
   int Kmax = 0;
   for (int i = 0; i < n; ++i) Kmax = std::max(Kmax, host_nstates[i]);
@@ -371,6 +373,34 @@ int Context::run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
   impute_chunks = (int)chunk_start.size() - 1;
   launch_impute_finish(panel, mc, w, d_hl, d_flat, d_hp, stream);
   prof.kernel_launches += 2;
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "imputation launch");
+  return GP_OK;
+}
+
+// The checkpointed variant (kernels_impute_ckpt.cu): checkpoint rows every 32
+// polymorphic sites (FP32 or BF16), recompute in the backward pass, FP64 chunk
+// log-likelihood per haplotype into d_loglik.
+int Context::run_impute_ckpt(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
+  ImputeWork& w = impute;
+  const int n = w.n, L = w.L;
+  const bool bf16 = precision_mode == GP_PRECISION_CKPT_BF16;
+  cudaError_t e;
+  if ((e = ckpt.ensure((size_t)n * w.WB * w.Kp * (bf16 ? 2 : 4))) != cudaSuccess) return cuda_fail(e, "alloc ckpt");
+  if ((e = ckpt_sum.ensure((size_t)n * w.WB * 4)) != cudaSuccess) return cuda_fail(e, "alloc ckpt");
+  if ((e = ckpt_scratch.ensure((size_t)n * 32 * w.Kp * 4)) != cudaSuccess) return cuda_fail(e, "alloc ckpt");
+  if ((e = loglik.ensure((size_t)n * 8)) != cudaSuccess) return cuda_fail(e, "alloc loglik");
+  launch_site_records(panel, mc, w, d_hl, d_flat, stream);
+  double cells = 0;
+  for (int i = 0; i < n; ++i) cells += (double)impute_np[i] * (double)host_nstates[i];
+  cudaEvent_t ea;
+  prof_begin(ea);
+  if (launch_impute_ckpt(w, bf16, ckpt.ptr, ckpt_sum.as<float>(), ckpt_scratch.as<float>(), loglik.as<double>(),
+                         d_hp, stream) != GP_OK)
+    return (fail(GP_E_ARG, "imputation: too many states"), GP_E_ARG);
+  prof_end(ea, 0, cells);
+  launch_impute_finish(panel, mc, w, d_hl, d_flat, d_hp, stream);
+  prof.kernel_launches += 3;
+  loglik_n = n;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "imputation launch");
   return GP_OK;
 }
@@ -562,6 +592,25 @@ int gp_ctx_destroy(gp_ctx* ctx) {
 
 const char* gp_last_error(const gp_ctx* ctx) {
   return ctx ? reinterpret_cast<const Context*>(ctx)->err.c_str() : "null context";
+}
+
+int gp_set_precision(gp_ctx* ctx, int32_t mode) {
+  if (!ctx) return GP_E_ARG;
+  Context& c = *reinterpret_cast<Context*>(ctx);
+  if (mode != GP_PRECISION_FULL && mode != GP_PRECISION_CKPT_F32 && mode != GP_PRECISION_CKPT_BF16)
+    return (c.fail(GP_E_ARG, "precision: unknown mode"), GP_E_ARG);
+  c.precision_mode = mode;
+  return GP_OK;
+}
+
+int gp_loglik_get(gp_ctx* ctx, int32_t n, double* out) {
+  if (!ctx || !out) return GP_E_ARG;
+  Context& c = *reinterpret_cast<Context*>(ctx);
+  if (c.loglik_n <= 0) return (c.fail(GP_E_STATE, "loglik: no checkpointed imputation has run"), GP_E_STATE);
+  if (n != c.loglik_n) return (c.fail(GP_E_ARG, "loglik: n differs from the last imputation call"), GP_E_ARG);
+  cudaMemcpyAsync(out, c.loglik.ptr, (size_t)n * 8, cudaMemcpyDeviceToHost, c.stream);
+  cudaError_t e = cudaStreamSynchronize(c.stream);
+  return e == cudaSuccess ? GP_OK : c.cuda_fail(e, "loglik_get");
 }
 
 int gp_impute_batch(gp_ctx* ctx, int32_t n, const int64_t* states_off, const uint32_t* states, const float* hl,

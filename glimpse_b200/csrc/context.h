@@ -103,6 +103,10 @@ struct Context {
   int build_condsets(int n, const std::vector<int64_t>& off, const std::vector<uint32_t>& states);
   int run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp);
   size_t store_budget(size_t held);
+  int run_impute_ckpt(const float* d_hl, const uint8_t* d_flat, float* d_hp);
+  int precision_mode = GP_PRECISION_FULL;
+  DevBuf ckpt, ckpt_sum, ckpt_scratch, loglik;  // checkpointed imputation (kernels_impute_ckpt.cu)
+  int loglik_n = 0;                             // entries of the last checkpointed imputation call
   int impute_chunks = 0;  // launches pairs of the last run_impute (1 when the whole batch fit)
   int set_targets(int n, const uint8_t* gl, const uint8_t* flat, const int32_t* ploidy, const int32_t* kp);
   int build_condsets_device(int n, int Kp);

@@ -106,6 +106,10 @@ int impute_groups(int Kmax);
 // Row stride (floats) of the forward-backward store for at most Kmax states; the
 // scratch split_scr holds round_up(2 n, 4) + n * stride floats.
 int impute_store_stride(int Kmax);
+// The checkpointed forward-backward (kernels_impute_ckpt.cu) over the batch's
+// conditioning sets: leaves prob_hid pairs in hp for k_impute_finish.
+int launch_impute_ckpt(ImputeWork& w, bool bf16, void* ckpt, float* csum, float* scratch, double* loglik, float* hp,
+                       cudaStream_t s);
 void launch_impute_finish(const DevPanel& P, const ModelConst& mc, ImputeWork& w, const float* hl,
                         const uint8_t* flat, float* hp, cudaStream_t s);
 

@@ -27,7 +27,9 @@ EXPORTS = [
     "gp_ligate_swap", "gp_gp_accum_get",
     "gp_mlp_param_count", "gp_mlp_init", "gp_mlp_set_params", "gp_mlp_get_params", "gp_mlp_forward",
     "gp_mlp_train_step", "gp_learned_enable", "gp_learned_train", "gp_learned_windows", "gp_state_posteriors",
+    "gp_set_precision", "gp_loglik_get",
 ]
+PRECISION_FULL, PRECISION_CKPT_F32, PRECISION_CKPT_BF16 = 0, 1, 2
 
 
 class gp_profile(C.Structure):
@@ -361,6 +363,16 @@ class Context:
         self._check(self.lib.gp_mlp_train_step(self.h, x.shape[0], _p(x, C.c_float), _p(y, C.c_float),
                                                _p(wt, C.c_float), C.c_float(lr), C.byref(loss), _p(g, C.c_float)))
         return loss.value, g
+
+    def set_precision(self, mode):
+        """gp_set_precision: PRECISION_FULL, PRECISION_CKPT_F32 or PRECISION_CKPT_BF16."""
+        self._check(self.lib.gp_set_precision(self.h, mode))
+
+    def loglik(self, n):
+        """gp_loglik_get: FP64 chunk log-likelihoods of the last checkpointed imputation call."""
+        out = np.zeros(n, np.float64)
+        self._check(self.lib.gp_loglik_get(self.h, n, _p(out, C.c_double)))
+        return out
 
     def learned_windows(self):
         n = self.lib.gp_learned_windows(self.h)

@@ -41,6 +41,11 @@ extern "C" {
 #define GP_MAX_TARGETS 32767
 #define GP_MAX_BATCH 65535
 
+/* Precision modes of the imputation forward-backward (gp_set_precision). */
+#define GP_PRECISION_FULL 0       /* every forward row kept in FP32, as the reference keeps them */
+#define GP_PRECISION_CKPT_F32 1   /* FP32 checkpoints every 32 sites, FP32 recompute, FP64 log-likelihood */
+#define GP_PRECISION_CKPT_BF16 2  /* BF16 checkpoints every 32 sites, FP32 recompute, FP64 log-likelihood */
+
 #define GP_STAGE_INIT 0
 #define GP_STAGE_BURN 1
 #define GP_STAGE_MAIN 2
@@ -200,6 +205,22 @@ int gp_impute_batch(gp_ctx* ctx, int32_t n, const int64_t* states_off, const uin
  * before any stream capture. Overlapping calls on one device race. */
 int gp_impute_one_static(gp_ctx* ctx, int32_t k, const uint32_t* states, const float* hl, const uint8_t* flat,
                          float* hp);
+
+/* Precision of the imputation forward-backward for every later call (no
+ * counterpart in the reference, which keeps every forward row,
+ * imputation_hmm.cpp:53-59). GP_PRECISION_FULL (the default) keeps all rows in
+ * FP32. The checkpointed modes keep the forward row after every 32nd
+ * polymorphic site only (FP32 or BF16; about 1/32 or 1/64 of the memory),
+ * recompute each block's rows in FP32 during the backward pass, and accumulate
+ * the chunk log-likelihood sum_l log AlphaSum_l in FP64 (gp_loglik_get). With
+ * FP32 checkpoints the posteriors are those of the same recursion without
+ * checkpoints; BF16 checkpoints trade a small posterior error for memory. */
+int gp_set_precision(gp_ctx* ctx, int32_t mode);
+
+/* The FP64 chunk log-likelihood of each haplotype of the last imputation call
+ * made in a checkpointed mode (n entries, in the call's order; for a Gibbs
+ * iteration: the targets' second haplotypes, or first for haploid targets). */
+int gp_loglik_get(gp_ctx* ctx, int32_t n, double* out);
 
 /* phasing_hmm::rephaseHaplotypes(H0, H1, flat) (phasing_hmm.h:136) for n
  * diploid targets with explicit conditioning sets; h0/h1 updated in place
