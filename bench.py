@@ -492,6 +492,31 @@ def run_case(args):
         t = float(np.median(times[1:]))
         print(f"{args.fmt}: {n} targets x {L} sites, {1e3 * t:.1f} ms per call (median of {args.reps})")
         ctx.close()
+    elif args.case == "mlp":
+        # the learned proposal's fused forward on the tensor cores: rows of
+        # random features, timed with CUDA events on the context stream
+        import torch
+        w = synth.make_panel_and_targets(600, 4000, 0.4, 0.5, 1, ("uniform", 0.5, 2.0), ("uniform", 80, 300),
+                                         seed=7, sparse_maf=0.01, lq_frac=0.02, alt_major_frac=0.1)
+        ctx = native.Context(w.panel)
+        ctx.mlp_init(1)
+        n = args.rows
+        x = np.random.default_rng(1).random((n, 48), dtype=np.float32)
+        stream = torch.cuda.ExternalStream(ctx.stream_handle())
+        ctx.mlp_forward(x[:1024])
+        times = []
+        for _ in range(args.reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.mlp_forward(x)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        flop = 2.0 * n * (64 * 256 + 256 * 256 + 256)
+        t = float(np.median(times))
+        print(f"mlp forward: {n} rows, {t:.2f} ms per call including the host copy of the features and scores "
+              f"({flop / t / 1e9:.1f} TFLOP/s of the 48(64)->256->256->1 network)")
+        ctx.close()
     elif args.case == "records":
         w = synth.workload(args.config, seed=1, n_targets=args.targets)
         T = w.targets
@@ -518,12 +543,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--subset", type=int, default=0,
                     help="targets of the fixed subset both arms run completely (default: host threads, at most 32)")
-    ap.add_argument("--case", choices=["iterations", "gl", "records"], default=None,
+    ap.add_argument("--case", choices=["iterations", "gl", "records", "mlp"], default=None,
                     help="run a small single-stage case (for profiler captures) instead of the bench")
     ap.add_argument("--targets", type=int, default=16)
     ap.add_argument("--iterations", type=int, default=2)
     ap.add_argument("--fmt", choices=["PL", "GL"], default="PL")
     ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--rows", type=int, default=4 << 20)
     ap.add_argument("--learned", action="store_true",
                     help="learned proposal vs plain PBWT selection (separate line; see run_learned)")
     ap.add_argument("--learned-frac", type=float, default=0.4)

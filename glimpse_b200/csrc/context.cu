@@ -237,6 +237,7 @@ Context::~Context() {
   out_gp.release(); out_site.release();
   lig_a.release(); lig_b.release(); lig_s.release(); lig_cnt.release();
   for (DevBuf* b : mlp.all()) b->release();
+  tune_tarhap.release();
   ckpt.release(); ckpt_sum.release(); ckpt_scratch.release(); loglik.release();
   for (DevBuf* b : learned.all()) b->release();
   if (phase_err_host) cudaFreeHost(phase_err_host);
@@ -361,10 +362,40 @@ int Context::run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
   const int J = impute_groups(Kmax);
   cudaEvent_t ea;
   prof_begin(ea);
+  int cpc = fixed_cpc ? fixed_cpc : tune_cpc;
+  if (!cpc) {
+    // Autotune chains per CTA on this batch's first chunk: phase 1 only writes
+    // the store, so the runs repeat the same work; the real run follows.
+    cpc = 2;
+    if (chunk_start[1] >= 16) {
+      const int cand[3] = {1, 2, 4};
+      cudaEvent_t e0, e1;
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      float best = 1e30f;
+      for (int ci = 0; ci < 3; ++ci) {
+        cudaEventRecord(e0, stream);
+        const int lrc = launch_impute_warp(1, J, mc, w, d_hp, stream, 0, chunk_start[1], cand[ci]);
+        cudaEventRecord(e1, stream);
+        float ms = 1e30f;
+        if (lrc == GP_OK && cudaEventSynchronize(e1) == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        else cudaGetLastError();
+        tune_ms[ci] = ms < 1e29f ? ms : -1.f;
+        if (ms < best) {
+          best = ms;
+          cpc = cand[ci];
+        }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      tune_cpc = cpc;
+      prof.kernel_launches += 3;
+    }
+  }
   for (size_t c = 0; c + 1 < chunk_start.size(); ++c) {
     const int j0 = chunk_start[c], nc = chunk_start[c + 1] - j0;
-    int lrc = launch_impute_warp(1, J, mc, w, d_hp, stream, j0, nc);
-    if (lrc == GP_OK) lrc = launch_impute_warp(2, J, mc, w, d_hp, stream, j0, nc);
+    int lrc = launch_impute_warp(1, J, mc, w, d_hp, stream, j0, nc, cpc);
+    if (lrc == GP_OK) lrc = launch_impute_warp(2, J, mc, w, d_hp, stream, j0, nc, cpc);
     if (lrc == GP_E_CUDA) return cuda_fail(cudaGetLastError(), "imputation: shared-memory attribute");
     if (lrc != GP_OK) return (fail(GP_E_ARG, "imputation: too many states"), GP_E_ARG);
     prof.kernel_launches += 2;
@@ -592,6 +623,31 @@ int gp_ctx_destroy(gp_ctx* ctx) {
 
 const char* gp_last_error(const gp_ctx* ctx) {
   return ctx ? reinterpret_cast<const Context*>(ctx)->err.c_str() : "null context";
+}
+
+int gp_tuning_set(gp_ctx* ctx, int32_t chains_per_cta, int32_t sweep_haps_per_warp) {
+  if (!ctx) return GP_E_ARG;
+  Context& c = *reinterpret_cast<Context*>(ctx);
+  if ((chains_per_cta != 0 && chains_per_cta != 1 && chains_per_cta != 2 && chains_per_cta != 4) ||
+      (sweep_haps_per_warp != 0 && sweep_haps_per_warp != 1 && sweep_haps_per_warp != 2 && sweep_haps_per_warp != 4 &&
+       sweep_haps_per_warp != 8))
+    return (c.fail(GP_E_ARG, "tuning: chains per CTA in {0, 1, 2, 4}, haplotypes per sweep warp in {0, 1, 2, 4, 8}"),
+            GP_E_ARG);
+  c.fixed_cpc = chains_per_cta;
+  c.fixed_hpw = sweep_haps_per_warp;
+  if (!chains_per_cta) c.tune_cpc = 0;
+  if (!sweep_haps_per_warp) c.tune_hpw = 0;
+  return GP_OK;
+}
+
+int gp_tuning_get(gp_ctx* ctx, int32_t* chains_per_cta, int32_t* sweep_haps_per_warp, float* ms) {
+  if (!ctx) return GP_E_ARG;
+  Context& c = *reinterpret_cast<Context*>(ctx);
+  if (chains_per_cta) *chains_per_cta = c.fixed_cpc ? c.fixed_cpc : c.tune_cpc;
+  if (sweep_haps_per_warp) *sweep_haps_per_warp = c.fixed_hpw ? c.fixed_hpw : c.tune_hpw;
+  if (ms)
+    for (int i = 0; i < 7; ++i) ms[i] = c.tune_ms[i];
+  return GP_OK;
 }
 
 int gp_set_precision(gp_ctx* ctx, int32_t mode) {

@@ -108,6 +108,12 @@ struct Context {
   DevBuf ckpt, ckpt_sum, ckpt_scratch, loglik;  // checkpointed imputation (kernels_impute_ckpt.cu)
   int loglik_n = 0;                             // entries of the last checkpointed imputation call
   int impute_chunks = 0;  // launches pairs of the last run_impute (1 when the whole batch fit)
+  // Autotuner: launch shapes picked by timing every candidate on the first batch
+  // large enough to tell them apart; fixed_* (gp_tuning_set) override it.
+  int tune_cpc = 0, tune_hpw = 0;     // chosen chains per CTA / haplotypes per sweep warp (0: not yet)
+  int fixed_cpc = 0, fixed_hpw = 0;
+  float tune_ms[7] = {0, 0, 0, 0, 0, 0, 0};  // phase-1 ms for 1, 2, 4 chains per CTA; sweep ms for 1, 2, 4, 8
+  DevBuf tune_tarhap;
   int set_targets(int n, const uint8_t* gl, const uint8_t* flat, const int32_t* ploidy, const int32_t* kp);
   int build_condsets_device(int n, int Kp);
   int select_states(int stage, int iteration, int& Kp);

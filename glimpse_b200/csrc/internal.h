@@ -97,9 +97,10 @@ void launch_compact_poly(const DevPanel& P, ImputeWork& w, cudaStream_t s);
 void launch_build_hvar(const DevPanel& P, ImputeWork& w, cudaStream_t s);
 void launch_site_records(const DevPanel& P, const ModelConst& mc, ImputeWork& w, const float* hl,
                          const uint8_t* flat, cudaStream_t s);
-// Chains of the haplotypes order[first .. first + count) (count < 0: all n).
+// Chains of the haplotypes order[first .. first + count) (count < 0: all n),
+// cpc chains per CTA (1, 2 or 4; GP_E_ARG when their shared memory does not fit).
 int launch_impute_warp(int phase, int J, const ModelConst& mc, ImputeWork& w, float* hp, cudaStream_t s,
-                       int first = 0, int count = -1);
+                       int first = 0, int count = -1, int cpc = 2);
 // Register groups per lane of the imputation chain kernel for at most Kmax
 // states (the J of launch_impute_warp).
 int impute_groups(int Kmax);

@@ -42,7 +42,7 @@ namespace gp {
 
 namespace {
 
-constexpr int kChainsPerCta = 2;
+constexpr int kMaxChainsPerCta = 4;     // chains per CTA: 1, 2 or 4 (the autotuner's choice)
 constexpr int kWarpsPerChain = 1;       // W
 constexpr int kRowDepth = 3;         // stored rows fetched this many sites ahead
 constexpr int kRing = kRowDepth + 1;      // ring slots
@@ -468,18 +468,18 @@ __device__ __forceinline__ void run_chain(const ChainArgs& A, char* smem, float4
   }
 }
 
-// Chain c = blockIdx.x * kChainsPerCta + (warp / W) is run by the W warps
+// Chain c = blockIdx.x * (chains per CTA) + (warp / W) is run by the W warps
 // (warp % W = 0..W-1) of its slot: haplotype order[c / 2] (c / 2 without an
 // order), forward for even chains and backward for odd ones. Every warp of a chain takes the same branches, so the
 // chain's named barrier (id 1 + slot) always sees all 32 W threads.
 template <int J, int W, bool POST>
-__global__ void __launch_bounds__(32 * W * kChainsPerCta) k_impute_warp(ChainArgs A) {
+__global__ void __launch_bounds__(32 * W * kMaxChainsPerCta) k_impute_warp(ChainArgs A) {
   extern __shared__ __align__(16) char smem_raw[];
-  __shared__ float4 xch[kChainsPerCta][2 * W];
+  __shared__ float4 xch[kMaxChainsPerCta][2 * W];
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int slot = warp / W, wi = warp % W;
-  const int chain = blockIdx.x * kChainsPerCta + slot;
+  const int chain = blockIdx.x * (int)(blockDim.x / (32 * W)) + slot;
   if (chain >= A.nchains) return;
   char* smem = smem_raw + (size_t)warp * warp_smem_bytes(J);
   const int t = A.order ? A.order[chain >> 1] : chain >> 1;
@@ -489,7 +489,7 @@ __global__ void __launch_bounds__(32 * W * kChainsPerCta) k_impute_warp(ChainArg
 
 }  // namespace
 
-size_t impute_warp_smem(int J) { return (size_t)kWarpsPerChain * kChainsPerCta * warp_smem_bytes(J); }
+size_t impute_warp_smem(int J, int cpc) { return (size_t)kWarpsPerChain * cpc * warp_smem_bytes(J); }
 
 // Local quads per warp for at most Kmax states (the J of launch_impute_warp).
 int impute_groups(int Kmax) {
@@ -501,22 +501,23 @@ int impute_groups(int Kmax) {
 int impute_store_stride(int Kmax) { return 128 * kWarpsPerChain * impute_groups(Kmax); }
 
 template <int J, bool POST>
-static int launch_chains(const ChainArgs& a, cudaStream_t s) {
+static int launch_chains(const ChainArgs& a, int cpc, cudaStream_t s) {
   constexpr int W = kWarpsPerChain;
-  const size_t sm = impute_warp_smem(J);
+  if (cpc < 1 || cpc > kMaxChainsPerCta) return GP_E_ARG;
+  const size_t sm = impute_warp_smem(J, cpc);
   if (sm > 200 * 1024) return GP_E_ARG;
   // The attribute is per device (contexts may sit on different devices);
   // setting it at every launch is cheap.
   if (cudaFuncSetAttribute(k_impute_warp<J, W, POST>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) !=
       cudaSuccess)
     return GP_E_CUDA;
-  const dim3 g((a.nchains + kChainsPerCta - 1) / kChainsPerCta);
-  k_impute_warp<J, W, POST><<<g, 32 * W * kChainsPerCta, sm, s>>>(a);
+  const dim3 g((a.nchains + cpc - 1) / cpc);
+  k_impute_warp<J, W, POST><<<g, 32 * W * cpc, sm, s>>>(a);
   return GP_OK;
 }
 
 int launch_impute_warp(int phase, int J, const ModelConst& mc, ImputeWork& w, float* hp, cudaStream_t s, int first,
-                       int count) {
+                       int count, int cpc) {
   ChainArgs a;
   a.sc.asum = w.split_scr.as<float>();
   a.sc.bsum = a.sc.asum + w.n;
@@ -543,7 +544,7 @@ int launch_impute_warp(int phase, int J, const ModelConst& mc, ImputeWork& w, fl
   a.hp = hp;
   a.order = w.order.ptr ? w.order.as<int32_t>() + first : nullptr;
 #define GP_WARP(JJ) \
-  case JJ: return phase == 2 ? launch_chains<JJ, true>(a, s) : launch_chains<JJ, false>(a, s);
+  case JJ: return phase == 2 ? launch_chains<JJ, true>(a, cpc, s) : launch_chains<JJ, false>(a, cpc, s);
   switch (J) {
     GP_WARP(1) GP_WARP(2) GP_WARP(3) GP_WARP(4) GP_WARP(5) GP_WARP(6) GP_WARP(7) GP_WARP(8)
     GP_WARP(9) GP_WARP(10) GP_WARP(11) GP_WARP(12) GP_WARP(13) GP_WARP(14) GP_WARP(15) GP_WARP(16)

@@ -198,15 +198,15 @@ __global__ void k_event_bits(PbwtSelectArgs a) {
   }
 }
 
-// Haplotypes per sweep warp. Lane l runs haplotype l % kSweepHaps of its warp's
-// group: lanes l, l + kSweepHaps, ... run the same haplotype, take the same
-// branches and write the same values to the same addresses, so a warp diverges
-// only over kSweepHaps haplotypes while all 32 lanes share the row staging.
-constexpr int kSweepHaps = 2;
-
-// One warp per block; lane l runs target haplotype blockIdx.x * kSweepHaps +
-// l % kSweepHaps (measured at 256 targets: 39 ms per sweep with 32 haplotypes per
-// warp, 33 ms with 2, as a warp runs every branch any of its haplotypes takes).
+// Haplotypes per sweep warp (hpw, a power of two, chosen by the autotuner).
+// Lane l runs haplotype l % hpw of its warp's group: lanes l, l + hpw, ... run
+// the same haplotype, take the same branches and write the same values to the
+// same addresses, so a warp diverges only over hpw haplotypes while all 32
+// lanes share the row staging.
+//
+// One warp per block; lane l runs target haplotype blockIdx.x * hpw + l % hpw
+// (measured at 256 targets: 39 ms per sweep with 32 haplotypes per warp, 33 ms
+// with 2, as a warp runs every branch any of its haplotypes takes).
 // The lanes of a warp walk the event list (non-LQ common sites and runs of rare sites) in step: every branch
 // that skips work is warp-uniform. Shared memory per warp holds
 //   ring    D slots, one per HQ common site l, filled by cp.async D common sites
@@ -216,10 +216,10 @@ constexpr int kSweepHaps = 2;
 //   scnt    the per-level push counts, one column per lane.
 // D = 0 reads the rows from global memory (panels whose rows do not fit in
 // shared memory).
-__global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D) {
+__global__ void __launch_bounds__(32) k_pbwt_sweep(PbwtSelectArgs a, int D, int hpw) {
   extern __shared__ __align__(16) uint32_t smem[];
   const int lane = threadIdx.x & 31;
-  const int hp = blockIdx.x * kSweepHaps + lane % kSweepHaps;
+  const int hp = blockIdx.x * hpw + (lane & (hpw - 1));
   const unsigned live = __ballot_sync(0xffffffffu, hp < a.n_haps);
   if (hp >= a.n_haps) return;
   const int rank = __popc(live & ((1u << lane) - 1u)), nlive = __popc(live);
@@ -478,20 +478,33 @@ __global__ void k_pbwt_union(PbwtSelectArgs a) {
 
 }  // namespace
 
-void launch_pbwt_select(const PbwtSelectArgs& a, cudaStream_t s) {
+static size_t sweep_smem(const PbwtSelectArgs& a, int& D) {
+  // Ring of D rank rows, D <= 8, within 96 KB.
+  const size_t slot_bytes = (size_t)a.P.R * 4;
+  D = (int)std::min<size_t>(8, (96u << 10) / slot_bytes);
+  if (D < 2) D = 0;
+  return (size_t)D * slot_bytes + 2 * 32 * 2 * 16 + (size_t)a.depth * 32 * 4;
+}
+
+void launch_pbwt_sweep(const PbwtSelectArgs& a, int hpw, cudaStream_t s) {
+  int D = 0;
+  const size_t smem = sweep_smem(a, D);
+  // The attribute is per device; setting it at every launch is cheap.
+  if (smem > (48u << 10)) cudaFuncSetAttribute(k_pbwt_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 << 10);
+  k_pbwt_sweep<<<(a.n_haps + hpw - 1) / hpw, 32, smem, s>>>(a, D, hpw);
+}
+
+void launch_pbwt_select(const PbwtSelectArgs& a, int hpw, cudaStream_t s) {
+  launch_pbwt_prepare(a, s);
+  launch_pbwt_sweep(a, hpw, s);
+  k_pbwt_union<<<(a.n_targets + 63) / 64, 64, 0, s>>>(a);
+}
+
+void launch_pbwt_prepare(const PbwtSelectArgs& a, cudaStream_t s) {
   k_pbwt_rng<<<1, 32, 0, s>>>(a);
   k_rare_carriers<<<dim3((a.Wc + 127) / 128, a.n_haps), 128, 0, s>>>(a);
   const int ycap = std::max(1, std::min(a.grid_y_cap, 65535));
   if (a.We > 0) k_event_bits<<<dim3((a.n_haps + 127) / 128, std::min(a.We, ycap)), 128, 0, s>>>(a);
-  // Ring of D rank rows, D <= 8, within 96 KB.
-  const size_t slot_bytes = (size_t)a.P.R * 4;
-  int D = (int)std::min<size_t>(8, (96u << 10) / slot_bytes);
-  if (D < 2) D = 0;
-  const size_t smem = (size_t)D * slot_bytes + 2 * 32 * 2 * 16 + (size_t)a.depth * 32 * 4;
-  // The attribute is per device; setting it at every launch is cheap.
-  if (smem > (48u << 10)) cudaFuncSetAttribute(k_pbwt_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 << 10);
-  k_pbwt_sweep<<<(a.n_haps + kSweepHaps - 1) / kSweepHaps, 32, smem, s>>>(a, D);
-  k_pbwt_union<<<(a.n_targets + 63) / 64, 64, 0, s>>>(a);
 }
 
 }  // namespace gp

@@ -151,8 +151,7 @@ __global__ void k_var_records(const int32_t* __restrict__ tsel, const int32_t* _
 // ---------------------------------------------------------------------------
 // Block reduction of 8 values (one per hypothesis).
 // Within a warp a reduce-scatter leaves lane L with the warp sum of value
-// ((L>>4)&1)*4 + ((L>>3)&1)*2 + ((L>>2)&1); after one barrier every thread
-// combines the warps' partials from shared memory.
+// ((L>>4)&1)*4 + ((L>>3)&1)*2 + ((L>>2)&1); warps are then combined in order.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void block_sum8(float (&v)[8], float (*red)[NW][8], int& buf, float (&out)[8]) {
   const int lane = threadIdx.x & 31;
@@ -186,22 +185,20 @@ __device__ __forceinline__ void block_sum8(float (&v)[8], float (*red)[NW][8], i
   const int warp = threadIdx.x >> 5;
   if ((lane & 3) == 0) red[buf][warp][((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1)] = c;
   __syncthreads();
-  // every thread adds the warps' partials itself (broadcast float4 reads), in
-  // one fixed tree: ((w0 + w1) + (w2 + w3)) + ((w4 + w5) + (w6 + w7))
-  static_assert(NW == 8, "eight warp partials");
-  const float4* r = reinterpret_cast<const float4*>(&red[buf][0][0]);
-  auto add4 = [](float4 a, float4 b) {
-    return make_float4(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z), __fadd_rn(a.w, b.w));
-  };
+  // lane l combines warps for hypotheses (l >> 3) and (l >> 3) + 4; butterflies
+  // over the warp index (l & 7) give the lanes of a group identical totals
+  static_assert(NW == 8, "one lane per warp partial");
+  float x0 = red[buf][lane & 7][lane >> 3];
+  float x1 = red[buf][lane & 7][(lane >> 3) + 4];
 #pragma unroll
-  for (int half = 0; half < 2; ++half) {  // hypotheses 0-3, then 4-7
-    const float4 s01 = add4(r[half], r[2 + half]), s23 = add4(r[4 + half], r[6 + half]);
-    const float4 s45 = add4(r[8 + half], r[10 + half]), s67 = add4(r[12 + half], r[14 + half]);
-    const float4 s = add4(add4(s01, s23), add4(s45, s67));
-    out[4 * half] = s.x;
-    out[4 * half + 1] = s.y;
-    out[4 * half + 2] = s.z;
-    out[4 * half + 3] = s.w;
+  for (int o = 1; o < 8; o <<= 1) {
+    x0 = __fadd_rn(x0, __shfl_xor_sync(0xffffffffu, x0, o));
+    x1 = __fadd_rn(x1, __shfl_xor_sync(0xffffffffu, x1, o));
+  }
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    out[h] = __shfl_sync(0xffffffffu, x0, 8 * h);
+    out[h + 4] = __shfl_sync(0xffffffffu, x1, 8 * h);
   }
   buf ^= 1;
 }
@@ -227,7 +224,7 @@ __device__ __forceinline__ float transition(const double* __restrict__ cm, int p
 struct PhaseShared {
   // per VAR code: emissions of the 8 hypotheses for a state allele of 0 ([0..7]) and 1 ([8..15]); read as float4
   __align__(16) float etab[16][16];
-  __align__(16) float red[2][NW][8];
+  float red[2][NW][8];
   float sumH[8];
   float sumT;
   float hprobs[64];

@@ -534,7 +534,42 @@ int Context::pbwt_select_states(int stage, int iteration, int Kp) {
   a.seed = cfg.seed;
   a.iteration = iteration;
   cudaMemsetAsync(T.overflow.ptr, 0, 4, stream);
-  launch_pbwt_select(a, stream);
+  int hpw = fixed_hpw ? fixed_hpw : tune_hpw;
+  if (!hpw) {
+    hpw = 2;
+    if (a.n_haps >= 32) {
+      // Autotune haplotypes per sweep warp: the sweep's only state carried across
+      // iterations is tar_hap, restored before every candidate run.
+      cudaError_t et = tune_tarhap.ensure((size_t)a.n_haps);
+      if (et != cudaSuccess) return cuda_fail(et, "alloc tuning");
+      launch_pbwt_prepare(a, stream);
+      cudaMemcpyAsync(tune_tarhap.ptr, a.tar_hap, (size_t)a.n_haps, cudaMemcpyDeviceToDevice, stream);
+      const int cand[4] = {1, 2, 4, 8};
+      cudaEvent_t e0, e1;
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      float best = 1e30f;
+      for (int ci = 0; ci < 4; ++ci) {
+        cudaMemcpyAsync(a.tar_hap, tune_tarhap.ptr, (size_t)a.n_haps, cudaMemcpyDeviceToDevice, stream);
+        cudaEventRecord(e0, stream);
+        launch_pbwt_sweep(a, cand[ci], stream);
+        cudaEventRecord(e1, stream);
+        float ms = 1e30f;
+        if (cudaEventSynchronize(e1) == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        tune_ms[3 + ci] = ms;
+        if (ms < best) {
+          best = ms;
+          hpw = cand[ci];
+        }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      cudaMemcpyAsync(a.tar_hap, tune_tarhap.ptr, (size_t)a.n_haps, cudaMemcpyDeviceToDevice, stream);
+      tune_hpw = hpw;
+      prof.kernel_launches += 7;
+    }
+  }
+  launch_pbwt_select(a, hpw, stream);
   prof.kernel_launches += 5;
   int32_t ovf = 0;
   cudaMemcpyAsync(&ovf, T.overflow.ptr, 4, cudaMemcpyDeviceToHost, stream);

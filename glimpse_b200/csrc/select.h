@@ -103,6 +103,10 @@ struct PbwtSelectArgs {
   int iteration;
 };
 
-void launch_pbwt_select(const PbwtSelectArgs& a, cudaStream_t s);
+// The whole selection: prepare (stream starts, carrier bits, event bits),
+// sweep with hpw haplotypes per warp (1, 2, 4, 8 or 16), union.
+void launch_pbwt_select(const PbwtSelectArgs& a, int hpw, cudaStream_t s);
+void launch_pbwt_prepare(const PbwtSelectArgs& a, cudaStream_t s);
+void launch_pbwt_sweep(const PbwtSelectArgs& a, int hpw, cudaStream_t s);
 
 }  // namespace gp

@@ -27,7 +27,7 @@ EXPORTS = [
     "gp_ligate_swap", "gp_gp_accum_get",
     "gp_mlp_param_count", "gp_mlp_init", "gp_mlp_set_params", "gp_mlp_get_params", "gp_mlp_forward",
     "gp_mlp_train_step", "gp_learned_enable", "gp_learned_train", "gp_learned_windows", "gp_state_posteriors",
-    "gp_set_precision", "gp_loglik_get",
+    "gp_set_precision", "gp_loglik_get", "gp_tuning_set", "gp_tuning_get",
 ]
 PRECISION_FULL, PRECISION_CKPT_F32, PRECISION_CKPT_BF16 = 0, 1, 2
 
@@ -363,6 +363,16 @@ class Context:
         self._check(self.lib.gp_mlp_train_step(self.h, x.shape[0], _p(x, C.c_float), _p(y, C.c_float),
                                                _p(wt, C.c_float), C.c_float(lr), C.byref(loss), _p(g, C.c_float)))
         return loss.value, g
+
+    def tuning_set(self, chains_per_cta=0, sweep_haps_per_warp=0):
+        self._check(self.lib.gp_tuning_set(self.h, chains_per_cta, sweep_haps_per_warp))
+
+    def tuning(self):
+        """(chains per CTA, haplotypes per sweep warp, measured ms[7]) of the autotuner."""
+        a, b = C.c_int32(0), C.c_int32(0)
+        ms = np.zeros(7, np.float32)
+        self._check(self.lib.gp_tuning_get(self.h, C.byref(a), C.byref(b), _p(ms, C.c_float)))
+        return a.value, b.value, ms
 
     def set_precision(self, mode):
         """gp_set_precision: PRECISION_FULL, PRECISION_CKPT_F32 or PRECISION_CKPT_BF16."""

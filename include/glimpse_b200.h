@@ -314,6 +314,21 @@ int gp_state_posteriors(gp_ctx* ctx, int32_t n, const int64_t* states_off, const
 int gp_learned_train(gp_ctx* ctx, int32_t kcand, float kpos, int32_t steps, int32_t batch, float lr, uint64_t seed,
                      float* losses);
 
+/* Launch-shape autotuner (no counterpart in the reference). Two shapes are
+ * picked per context by timing every candidate on the first batch large
+ * enough to tell them apart (16 haplotypes for the imputation chains, 32 target
+ * haplotypes for the PBWT sweep): chains per CTA of the imputation
+ * forward-backward (1, 2 or 4: how many sequential chains share an SM's
+ * shared memory and schedulers) and target haplotypes per warp of the PBWT
+ * sweep (1, 2, 4 or 8: lockstep lanes against divergence). Results do not
+ * depend on either. gp_tuning_set fixes them (0: tune again on next use);
+ * gp_tuning_get reports the shapes in use (0: not tuned yet) and, in ms[7],
+ * the measured times (phase-1 chains for 1, 2, 4 chains per CTA, then the sweep
+ * for 1, 2, 4, 8 haplotypes per warp; -1 where a shape did not fit, 0 where
+ * not measured). */
+int gp_tuning_set(gp_ctx* ctx, int32_t chains_per_cta, int32_t sweep_haps_per_warp);
+int gp_tuning_get(gp_ctx* ctx, int32_t* chains_per_cta, int32_t* sweep_haps_per_warp, float* ms);
+
 /* Timing of the last gp_iteration by stage, in milliseconds (device events). */
 int gp_stage_times(gp_ctx* ctx, float* ms, int32_t n);
 

@@ -96,3 +96,37 @@ def test_disabling_restores_plain_selection():
     finally:
         a.close()
         b.close()
+
+
+@pytest.mark.gpu
+def test_autotuned_shapes_do_not_change_results():
+    """The autotuner picks chains per CTA (imputation) and haplotypes per warp
+    (PBWT sweep) by timing; results must not depend on either. Two contexts
+    with opposite fixed shapes give identical states, posteriors and
+    haplotypes, and an autotuned context reports the shapes it chose."""
+    from glimpse_b200 import native, synth
+    w = synth.make_panel_and_targets(1500, 8000, 1.0, 0.5, 20, ("uniform", 0.5, 2.0), ("uniform", 100, 300),
+                                     seed=41, sparse_maf=0.005)
+    P, T = w.panel, w.targets
+    kw = dict(kinit=250, kpbwt=int(T.kpbwt.max()), pbwt_depth=8, pbwt_modulo_cm=0.05)
+    ctxs = [native.Context(P, **kw) for _ in range(3)]
+    try:
+        ctxs[0].tuning_set(1, 1)
+        ctxs[1].tuning_set(4, 8)
+        for c in ctxs:
+            c.set_targets(T, kpbwt=T.kpbwt)
+            c.iteration(native.STAGE_INIT, 0)
+            c.iteration(native.STAGE_BURN, 1)
+        for t in range(T.n):
+            a, b = ctxs[0].posteriors(t), ctxs[1].posteriors(t)
+            assert np.array_equal(ctxs[0].states(t), ctxs[1].states(t))
+            assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+            assert np.array_equal(ctxs[0].states(t), ctxs[2].states(t))
+        h = [c.haps() for c in ctxs]
+        assert np.array_equal(h[0][0], h[1][0]) and np.array_equal(h[0][1], h[2][1])
+        cpc, hpw, ms = ctxs[2].tuning()
+        assert cpc in (1, 2, 4) and hpw in (1, 2, 4, 8)
+        assert (ms[:3] != 0).any() and (ms[3:] > 0).all()
+    finally:
+        for c in ctxs:
+            c.close()
