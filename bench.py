@@ -502,20 +502,17 @@ def run_case(args):
         ctx.mlp_init(1)
         n = args.rows
         x = np.random.default_rng(1).random((n, 48), dtype=np.float32)
-        stream = torch.cuda.ExternalStream(ctx.stream_handle())
         ctx.mlp_forward(x[:1024])
-        times = []
+        ctx.profile_reset()
         for _ in range(args.reps):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
             ctx.mlp_forward(x)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            times.append(e0.elapsed_time(e1))
-        flop = 2.0 * n * (64 * 256 + 256 * 256 + 256)
-        t = float(np.median(times))
-        print(f"mlp forward: {n} rows, {t:.2f} ms per call including the host copy of the features and scores "
-              f"({flop / t / 1e9:.1f} TFLOP/s of the 48(64)->256->256->1 network)")
+        p = ctx.profile()
+        t = (p["mlp_ms"] - 0.0) / max(1, p["mlp_launches"])
+        rows = p["mlp_rows"] / max(1, p["mlp_launches"])
+        # device time of the fused forward alone (CUDA events around each launch)
+        flop = 2.0 * rows * (64 * 256 + 256 * 256 + 256)
+        print(f"mlp forward: {rows:.0f} rows per launch (mean over {p['mlp_launches']} launches), {t:.3f} ms, "
+              f"{flop / t / 1e9:.1f} TFLOP/s of the 48(64)->256->256->1 network")
         ctx.close()
     elif args.case == "records":
         w = synth.workload(args.config, seed=1, n_targets=args.targets)

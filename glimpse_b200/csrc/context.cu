@@ -77,6 +77,10 @@ void Context::prof_resolve() {
         prof.phase_ms += ms;
         prof.phase_cells += p.cells;
         prof.phase_launches++;
+      } else if (p.kind == 3) {
+        prof.mlp_ms += ms;
+        prof.mlp_rows += p.cells;
+        prof.mlp_launches++;
       } else {
         prof.select_ms += ms;
       }

@@ -86,7 +86,7 @@ struct Context {
   // profiling: events around the hot kernels, resolved at the next host sync
   struct ProfEv {
     cudaEvent_t a, b;
-    int kind;  // 0 imputation forward-backward, 1 phasing, 2 selection
+    int kind;  // 0 imputation forward-backward, 1 phasing, 2 selection, 3 network forward
     double cells;
   };
   std::vector<ProfEv> prof_pending;

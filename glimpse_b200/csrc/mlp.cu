@@ -502,7 +502,10 @@ int mlp_forward_device(Context& c, const __nv_bfloat16* x, int n, float* score, 
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaEvent_t ea;
+  c.prof_begin(ea);
   cudaError_t e = launch_mlp_fwd(a, sms, c.stream);
+  c.prof_end(ea, 3, (double)n);
   c.prof.kernel_launches += 1;
   return e == cudaSuccess ? GP_OK : c.cuda_fail(e, "mlp forward launch");
 }

@@ -37,6 +37,7 @@ class gp_profile(C.Structure):
         ("impute_ms", C.c_double), ("impute_cells", C.c_double), ("impute_bytes", C.c_double),
         ("phase_ms", C.c_double), ("phase_cells", C.c_double), ("select_ms", C.c_double),
         ("impute_launches", C.c_int64), ("phase_launches", C.c_int64), ("kernel_launches", C.c_int64),
+        ("mlp_ms", C.c_double), ("mlp_rows", C.c_double), ("mlp_launches", C.c_int64),
     ]
 
 

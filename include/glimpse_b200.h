@@ -341,6 +341,8 @@ typedef struct gp_profile {
   double phase_ms, phase_cells;                  /* cells = VAR sites x states x 8 hypotheses, both passes */
   double select_ms;
   int64_t impute_launches, phase_launches, kernel_launches;
+  double mlp_ms, mlp_rows;                       /* the learned proposal's fused forward (k_mlp_fwd) */
+  int64_t mlp_launches;
 } gp_profile;
 int gp_profile_get(gp_ctx* ctx, gp_profile* out);
 int gp_profile_reset(gp_ctx* ctx);
