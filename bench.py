@@ -492,6 +492,54 @@ def run_case(args):
         t = float(np.median(times[1:]))
         print(f"{args.fmt}: {n} targets x {L} sites, {1e3 * t:.1f} ms per call (median of {args.reps})")
         ctx.close()
+    elif args.case == "groups":
+        # the workload's targets split over G contexts (one stream each) driven
+        # by G host threads: complete runs, device-timed from the first stream
+        import threading
+        import torch
+        w = synth.workload(args.config, seed=1)
+        T = w.targets
+        G = args.groups
+        parts = np.array_split(np.arange(T.n), G)
+        ctxs = []
+        for idx in parts:
+            sub = subset(T, T.n)
+            for k in ("ploidy", "gl", "flat", "truth", "kpbwt", "coverage"):
+                setattr(sub, k, getattr(T, k)[idx])
+            sub.n = len(idx)
+            c = native.Context(w.panel, kinit=w.params["kinit"], kpbwt=int(T.kpbwt.max()))
+            c.set_targets(sub, kpbwt=sub.kpbwt)
+            ctxs.append(c)
+        streams = [torch.cuda.ExternalStream(c.stream_handle()) for c in ctxs]
+
+        def one(c):
+            c.targets_reset()
+            c.run(BURNIN, MAIN)
+
+        def step():
+            th = [threading.Thread(target=one, args=(c,)) for c in ctxs]
+            for x in th:
+                x.start()
+            for x in th:
+                x.join()
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(streams[0])
+        for _ in range(args.steps):
+            step()
+        for st in streams[1:]:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            streams[0].wait_event(ev)
+        e1.record(streams[0])
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        print(f"groups={G}: {T.n} targets, {ms:.1f} ms per complete run, {T.n / (ms / 1000.0):.2f} samples/s")
+        for c in ctxs:
+            c.close()
     elif args.case == "mlp":
         # the learned proposal's fused forward on the tensor cores: rows of
         # random features, timed with CUDA events on the context stream
@@ -540,13 +588,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--subset", type=int, default=0,
                     help="targets of the fixed subset both arms run completely (default: host threads, at most 32)")
-    ap.add_argument("--case", choices=["iterations", "gl", "records", "mlp"], default=None,
+    ap.add_argument("--case", choices=["iterations", "gl", "records", "mlp", "groups"], default=None,
                     help="run a small single-stage case (for profiler captures) instead of the bench")
     ap.add_argument("--targets", type=int, default=16)
     ap.add_argument("--iterations", type=int, default=2)
     ap.add_argument("--fmt", choices=["PL", "GL"], default="PL")
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--rows", type=int, default=4 << 20)
+    ap.add_argument("--groups", type=int, default=2)
     ap.add_argument("--learned", action="store_true",
                     help="learned proposal vs plain PBWT selection (separate line; see run_learned)")
     ap.add_argument("--learned-frac", type=float, default=0.4)

@@ -459,6 +459,7 @@ __global__ void k_pbwt_union(PbwtSelectArgs a) {
       const uint32_t m = 1u << (h & 31);
       if (!(bm[h >> 5] & m)) {
         bm[h >> 5] |= m;
+        if (a.union_rank) a.union_rank[(size_t)t * N + h] = (lv << 16) | min(count, 0xFFFF);
         ++count;
       }
     }

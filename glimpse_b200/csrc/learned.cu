@@ -79,6 +79,8 @@ struct FeatArgs {
   const uint32_t* cand;
   const int32_t* ncand;
   const int32_t* kfinal;
+  const int32_t* urank;  // [n][N]: PBWT level << 16 | insertion index of the candidate in the union
+  int N, depth;
   __nv_bfloat16* x;  // rows ((t * nwin + w) * Kpc + k), kMlpInP columns
 };
 
@@ -223,12 +225,13 @@ __global__ void __launch_bounds__(128) k_features(FeatArgs a) {
     f[39] = ncf[4] / (float)kWinSites;
     f[40] = (float)w / (float)a.nwin;
     f[41] = log2f((float)max(1, a.kfinal[t])) / 11.f;
-    f[42] = present / 5.f;
+    const int ur = a.urank[(size_t)t * a.N + c];
+    f[42] = (float)(ur >> 16) / (float)a.depth;  // PBWT level of the candidate's first push
     f[43] = expf(-hom_mm);
     f[44] = expf(-hom_mm3);
     f[45] = het;
     f[46] = het_m;
-    f[47] = 1.f;
+    f[47] = (float)(ur & 0xFFFF) / (float)a.Kpc;  // its rank in the PBWT union order
   }
   uint4* dst = reinterpret_cast<uint4*>(row);
 #pragma unroll
@@ -556,6 +559,8 @@ int Context::learned_features(int Kpc, DevBuf& xout) {
   if ((e = lw.planes.ensure((size_t)n * kPlanes * W * 4)) != cudaSuccess) return cuda_fail(e, "learned alloc");
   const size_t rows = (size_t)n * lw.nwin * Kpc;
   if ((e = xout.ensure(rows * kMlpInP * 2)) != cudaSuccess) return cuda_fail(e, "learned features alloc");
+  if ((e = lw.urank.ensure((size_t)n * host.N * 4)) != cudaSuccess) return cuda_fail(e, "learned alloc");
+  if (!pbwt_active) cudaMemsetAsync(lw.urank.ptr, 0, (size_t)n * host.N * 4, stream);  // whole panel: no union
   cudaMemcpyAsync(lw.cand.ptr, w.states.ptr, (size_t)n * Kpc * 4, cudaMemcpyDeviceToDevice, stream);
   cudaMemcpyAsync(lw.ncand.ptr, w.nstates.ptr, (size_t)n * 4, cudaMemcpyDeviceToDevice, stream);
   k_pack_targets<<<dim3((W + 127) / 128, n), 128, 0, stream>>>(T.h0.as<uint8_t>(), T.h1.as<uint8_t>(),
@@ -572,6 +577,9 @@ int Context::learned_features(int Kpc, DevBuf& xout) {
   fa.cand = lw.cand.as<uint32_t>();
   fa.ncand = lw.ncand.as<int32_t>();
   fa.kfinal = lw.d_kfinal.as<int32_t>();
+  fa.urank = lw.urank.as<int32_t>();
+  fa.N = host.N;
+  fa.depth = cfg.pbwt_depth;
   fa.x = xout.as<__nv_bfloat16>();
   k_features<<<dim3((Kpc + 127) / 128, lw.nwin, n), 128, 0, stream>>>(fa);
   prof.kernel_launches += 2;

@@ -25,10 +25,11 @@ struct LearnedWork {
   std::vector<int32_t> kfinal;         // conditioning-set size per target (the caller's Kpbwt)
   DevBuf d_kfinal, planes, cand, ncand, x, score, best, cnt, site_win, nsites, mass0, mass1, astore, aoff;
   DevBuf xall, yall, wall, idx;
+  DevBuf urank;                        // [n][N]: PBWT level << 16 | insertion index of every union member
   int nwin = 0;
   std::vector<DevBuf*> all() {
     return {&d_kfinal, &planes, &cand, &ncand, &x, &score, &best, &cnt, &site_win, &nsites, &mass0, &mass1,
-            &astore, &aoff, &xall, &yall, &wall, &idx};
+            &astore, &aoff, &xall, &yall, &wall, &idx, &urank};
   }
 };
 

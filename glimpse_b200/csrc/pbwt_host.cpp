@@ -528,6 +528,12 @@ int Context::pbwt_select_states(int stage, int iteration, int Kp) {
   a.overflow = T.overflow.as<int32_t>();
   a.kpbwt = T.d_kpbwt.as<int32_t>();
   a.bitmap = T.bitmap.as<uint32_t>();
+  a.union_rank = nullptr;
+  if (learned.on) {
+    cudaError_t eu = learned.urank.ensure((size_t)T.n * host.N * 4);
+    if (eu != cudaSuccess) return cuda_fail(eu, "alloc union ranks");
+    a.union_rank = learned.urank.as<int32_t>();
+  }
   a.states = w.states.as<uint32_t>();
   a.nstates = w.nstates.as<int32_t>();
   a.Kp = Kp;

@@ -96,6 +96,7 @@ struct PbwtSelectArgs {
   int32_t* overflow;          // [1]
   const int32_t* kpbwt;       // [n_targets] (already min'ed with N)
   uint32_t* bitmap;           // [n_targets][ceil(N/32)]
+  int32_t* union_rank;        // [n_targets][N] or null: for every id the union inserts, level << 16 | insertion index
   uint32_t* states;           // [n_targets][Kp]
   int32_t* nstates;
   int Kp;

@@ -279,9 +279,10 @@ int gp_mlp_train_step(gp_ctx* ctx, int32_t n, const float* x, const float* y, co
  * conditioning_set::compactSelection (conditioning_set.cpp:96-104): the PBWT
  * selection (haplotype_set.cpp:317-728) runs with kcand states per target to
  * give candidates; every (target, window of 256 common sites, candidate) gets
- * 48 features (matches with the target's two current haplotypes over the
- * window and its neighbours, match runs through the window, agreement with
- * confident genotype-likelihood calls, densities); the network scores them;
+ * 48 features (the candidate's PBWT level and rank in the PBWT union order,
+ * matches with the target's two current haplotypes over the window and its
+ * neighbours, match runs through the window, agreement with confident
+ * genotype-likelihood calls, densities); the network scores them;
  * per window the top 32 candidates are ranked, and the conditioning set is the
  * union in rank order cut at the target's Kpbwt (gp_targets_set). The init
  * stage is unchanged. Disabled (the default), selection is the plain PBWT path.
