@@ -663,8 +663,9 @@ int gp_mlp_forward(gp_ctx* ctx, int32_t n, const float* x, float* score, float* 
   int rc = stage_rows(c, n, x, rows);
   if (rc != GP_OK) return rc;
   gp::MlpState& M = c.mlp;
-  rc = gp::mlp_forward_device(c, M.x.as<__nv_bfloat16>(), n, M.score.as<float>(), M.h1.as<__nv_bfloat16>(),
-                              M.h2.as<__nv_bfloat16>());
+  // the hidden activations are written only when the caller asks for them
+  rc = gp::mlp_forward_device(c, M.x.as<__nv_bfloat16>(), n, M.score.as<float>(),
+                              h1 ? M.h1.as<__nv_bfloat16>() : nullptr, h2 ? M.h2.as<__nv_bfloat16>() : nullptr);
   if (rc != GP_OK) return rc;
   cudaMemcpyAsync(score, M.score.ptr, (size_t)n * 4, cudaMemcpyDeviceToHost, c.stream);
   std::vector<__nv_bfloat16> hb;
