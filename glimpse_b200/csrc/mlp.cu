@@ -39,7 +39,8 @@ constexpr uint32_t kSmemH = kSmemX + kTileM * kMlpInP * 2;      // +16 KB
 constexpr uint32_t kSmemB1 = kSmemH + kTileM * 128 * 2;         // +32 KB (one K half of the hidden tile)
 constexpr uint32_t kSmemB2 = kSmemB1 + kMlpHid * 4;
 constexpr uint32_t kSmemW3 = kSmemB2 + kMlpHid * 4;
-constexpr uint32_t kSmemBar = kSmemW3 + kMlpHid * 4;
+constexpr uint32_t kSmemPart = kSmemW3 + kMlpHid * 4;  // the two halves' partial dot products
+constexpr uint32_t kSmemBar = kSmemPart + 256 * 4;
 constexpr uint32_t kSmemFwd = kSmemBar + 64;
 
 // cp.async of a row-major BF16 matrix [rows][kext] (K contiguous, row stride ld
@@ -56,7 +57,10 @@ __device__ __forceinline__ void stage_kmajor(uint8_t* tile, const __nv_bfloat16*
   }
 }
 
-__global__ void __launch_bounds__(128, 1) k_mlp_fwd(MlpFwdArgs a) {
+constexpr int kFwdThreads = 256;  // warps w and w + 4 share tensor-memory lanes 32 (w % 4) .. + 31 (the tile's
+                                  // rows) and split the columns of every epilogue step between them
+
+__global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd(MlpFwdArgs a) {
   extern __shared__ __align__(1024) uint8_t sm[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kSmemBar);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kSmemBar + 8);
@@ -64,7 +68,10 @@ __global__ void __launch_bounds__(128, 1) k_mlp_fwd(MlpFwdArgs a) {
   float* b1s = reinterpret_cast<float*>(sm + kSmemB1);
   float* b2s = reinterpret_cast<float*>(sm + kSmemB2);
   float* w3s = reinterpret_cast<float*>(sm + kSmemW3);
+  float* part = reinterpret_cast<float*>(sm + kSmemPart);
   const int tid = threadIdx.x, warp = tid >> 5;
+  const int trow = tid & (kTileM - 1);  // the tile row (tensor-memory lane) this thread reads
+  const int chalf = tid >> 7;           // which half of each epilogue step's columns it takes
   const int ntiles = (a.n + kTileM - 1) / kTileM;
   if ((int)blockIdx.x >= ntiles) return;
 
@@ -89,7 +96,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_fwd(MlpFwdArgs a) {
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tbase = *tslot;
-  const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+  const uint32_t lane_off = (uint32_t)((warp & 3) * 32) << 16;
   const uint32_t sW1 = tc::smem_u32(sm + kSmemW1), sW2 = tc::smem_u32(sm + kSmemW2);
   const uint32_t sX = tc::smem_u32(sm + kSmemX), sH = tc::smem_u32(sm + kSmemH);
   constexpr uint32_t idesc = tc::idesc_bf16(kTileM, kMlpHid);
@@ -105,7 +112,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_fwd(MlpFwdArgs a) {
 
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int r0 = tile * kTileM;
-    const int row = r0 + tid;
+    const int row = r0 + trow;
     stage_kmajor(sm + kSmemX, a.x + (size_t)r0 * kMlpInP, kTileM, kMlpInP, kMlpInP, a.n - r0, 0, kMlpInP);
     tc::cp_async_commit();
     tc::cp_async_wait<0>();
@@ -122,23 +129,25 @@ __global__ void __launch_bounds__(128, 1) k_mlp_fwd(MlpFwdArgs a) {
     if (!wait_mma()) break;
     bool ok = true;
     for (int h = 0; h < 2 && ok; ++h) {
-      // layer-1 epilogue for hidden units [128 h, 128 h + 128): bias, ReLU, BF16
+      // layer-1 epilogue for hidden units [128 h, 128 h + 128): bias, ReLU, BF16;
+      // this thread takes 64 of them
 #pragma unroll 1
-      for (int c = 0; c < 4; ++c) {
+      for (int c = 0; c < 2; ++c) {
+        const int c0 = chalf * 64 + c * 32;  // column within the half
         float v[32];
-        tc::tmem_ld32(tbase + lane_off + h * 128 + c * 32, v);
+        tc::tmem_ld32(tbase + lane_off + h * 128 + c0, v);
         uint32_t p[16];
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
-          const int j = h * 128 + c * 32 + 2 * i;
+          const int j = h * 128 + c0 + 2 * i;
           p[i] = tc::pack_bf16(fmaxf(v[2 * i] + b1s[j], 0.f), fmaxf(v[2 * i + 1] + b1s[j + 1], 0.f));
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const uint4 u = make_uint4(p[4 * q], p[4 * q + 1], p[4 * q + 2], p[4 * q + 3]);
-          *reinterpret_cast<uint4*>(sm + kSmemH + tc::kmajor_off(tid, c * 32 + q * 8, 128)) = u;
+          *reinterpret_cast<uint4*>(sm + kSmemH + tc::kmajor_off(trow, c0 + q * 8, 128)) = u;
           if (a.h1 && row < a.n)
-            *reinterpret_cast<uint4*>(a.h1 + (size_t)row * kMlpHid + h * 128 + c * 32 + q * 8) = u;
+            *reinterpret_cast<uint4*>(a.h1 + (size_t)row * kMlpHid + h * 128 + c0 + q * 8) = u;
         }
       }
       tc::fence_proxy_async();
@@ -155,10 +164,11 @@ __global__ void __launch_bounds__(128, 1) k_mlp_fwd(MlpFwdArgs a) {
       ok = wait_mma();
     }
     if (!ok) break;
-    // layer-2 epilogue: bias, ReLU, dot with w3 (FP32, in column order)
+    // layer-2 epilogue: bias, ReLU, dot with w3 in FP32 (this thread: 128 of the
+    // 256 columns in order; the two halves are added below)
     float acc = 0.f;
 #pragma unroll 1
-    for (int c = 0; c < 8; ++c) {
+    for (int c = chalf * 4; c < chalf * 4 + 4; ++c) {
       float v[32];
       tc::tmem_ld32(tbase + lane_off + 256 + c * 32, v);
       uint32_t p[16];
@@ -177,9 +187,10 @@ __global__ void __launch_bounds__(128, 1) k_mlp_fwd(MlpFwdArgs a) {
               make_uint4(p[4 * q], p[4 * q + 1], p[4 * q + 2], p[4 * q + 3]);
       }
     }
-    if (row < a.n) a.score[row] = acc + b3;
+    part[tid] = acc;
     tc::fence_before_sync();
     __syncthreads();
+    if (chalf == 0 && row < a.n) a.score[row] = (part[trow] + part[trow + kTileM]) + b3;
   }
   if (*abort_flag && tid == 0) atomicExch(a.err, 1);
   tc::fence_before_sync();
@@ -399,7 +410,7 @@ cudaError_t launch_mlp_fwd(const MlpFwdArgs& a, int grid, cudaStream_t s) {
   grid = std::max(1, std::min(grid, ntiles));
   cudaError_t e = cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemFwd);
   if (e != cudaSuccess) return e;
-  k_mlp_fwd<<<grid, 128, kSmemFwd, s>>>(a);
+  k_mlp_fwd<<<grid, kFwdThreads, kSmemFwd, s>>>(a);
   return cudaGetLastError();
 }
 
