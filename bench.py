@@ -388,8 +388,11 @@ def run_learned(args):
     simulated targets of the same panel (their own plain init and burn-in
     iterations give the haplotypes; labels are the HMM's window posteriors over
     their PBWT candidates). Reported: samples/s and dosage r2 of plain selection
-    at the workload's K, plain at K x --learned-frac, and the learned proposal at
-    K x --learned-frac (candidates: PBWT at the workload's K)."""
+    at the workload's K, plain at K x --learned-frac, the learned proposal at
+    K x --learned-frac, and the learned proposal sizing each target's set itself
+    (at most the workload's K); candidates: PBWT at the workload's largest K.
+    `value` is the last: learned + batched, matched when its r2 is within 0.002
+    of plain at the workload's K."""
     import torch
     from glimpse_b200 import native
     torch.cuda.set_device(0)
@@ -414,9 +417,10 @@ def run_learned(args):
     losses = ctx.learned_train(kcand=kcand, kpos=8.0, steps=args.train_steps, batch=16384, lr=1e-3, seed=7)
     t_train = time.perf_counter() - t0
 
-    def timed_runs(kp, learned):
+    def timed_runs(kp, learned, min_prob=0.5, kmin=0):
         ctx.learned_enable(False, kcand=kcand)
         ctx.set_targets(test, kpbwt=kp)
+        ctx.learned_size(min_prob, kmin)
         if learned:
             ctx.learned_enable(True, kcand=kcand)
         for _ in range(args.warmup):
@@ -432,22 +436,28 @@ def run_learned(args):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / args.steps
         _, _, ds, _, _ = ctx.gp()
+        kused = float(np.mean([ctx.states(t).size for t in range(test.n)]))  # last iteration's set sizes
         return {"samples_per_s": test.n / (ms / 1000.0), "ms_per_run": ms,
-                "dosage_r2": synth.dosage_r2(ds, test.truth.sum(1)), "k_mean": float(np.mean(kp))}
+                "dosage_r2": synth.dosage_r2(ds, test.truth.sum(1)), "k_mean": kused}
 
     plain_big = timed_runs(kbig, False)
     plain_small = timed_runs(ksmall, False)
     learned_small = timed_runs(ksmall, True)
+    # the network also sizes the sets: candidates some window scores at 0.5 or
+    # more, at least 32, at most the workload's K
+    learned_adaptive = timed_runs(kbig, True, 0.5, 32)
+    ctx.learned_size(0.5, 0)
     ctx.close()
-    matched = abs(learned_small["dosage_r2"] - plain_big["dosage_r2"]) <= 0.002
+    matched = abs(learned_adaptive["dosage_r2"] - plain_big["dosage_r2"]) <= 0.002
     line = {"metric": "samples/s at matched dosage r2 (learned + batched vs plain)", "unit": "samples/s",
-            "value": learned_small["samples_per_s"], "higher_is_better": True, "n_gpus": 1, "steps": args.steps,
+            "value": learned_adaptive["samples_per_s"], "higher_is_better": True, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "dtype": "f32 HMM, bf16 network", "data": "synthetic",
             "config": {"workload": args.config, "targets": test.n, "training_targets": train.n,
                        "training_steps": args.train_steps, "candidates_per_target": kcand,
                        "k_fraction": args.learned_frac},
             "plain_workload_k": plain_big, "plain_small_k": plain_small, "learned_small_k": learned_small,
-            "matched_r2": matched, "speedup_vs_plain": learned_small["samples_per_s"] / plain_big["samples_per_s"],
+            "learned_adaptive_k": learned_adaptive,
+            "matched_r2": matched, "speedup_vs_plain": learned_adaptive["samples_per_s"] / plain_big["samples_per_s"],
             "r2_gain_vs_plain_same_k": learned_small["dosage_r2"] - plain_small["dosage_r2"],
             "training": {"seconds": t_train, "loss_first": float(losses[:10].mean()),
                          "loss_last": float(losses[-10:].mean())}}

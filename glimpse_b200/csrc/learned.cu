@@ -418,9 +418,16 @@ __global__ void k_gather_rows(const __nv_bfloat16* __restrict__ xall, const floa
 // Per (target, window): the top kTopR candidates by score, one block argmax per
 // rank; best[t][k] keeps a candidate's best rank over windows, cnt[t][k] the
 // number of windows that ranked it.
+// Order-preserving map of a float to an int (for atomicMax over scores).
+__device__ __forceinline__ int fkey(float v) {
+  const int b = __float_as_int(v);
+  return b >= 0 ? b : b ^ 0x7FFFFFFF;
+}
+__device__ __forceinline__ float fval(int k) { return __int_as_float(k >= 0 ? k : k ^ 0x7FFFFFFF); }
+
 __global__ void __launch_bounds__(256) k_window_topr(const float* __restrict__ score, const int32_t* __restrict__ ncand,
                                                      int nwin, int Kpc, int32_t* __restrict__ best,
-                                                     int32_t* __restrict__ cnt) {
+                                                     int32_t* __restrict__ cnt, int32_t* __restrict__ maxs) {
   __shared__ float sc[kMaxCand];
   __shared__ float rv[8];
   __shared__ int rk[8];
@@ -462,6 +469,7 @@ __global__ void __launch_bounds__(256) k_window_topr(const float* __restrict__ s
       if (v > -INFINITY && kk < nc) {
         atomicMin(&best[(size_t)t * Kpc + kk], r);
         atomicAdd(&cnt[(size_t)t * Kpc + kk], 1);
+        atomicMax(&maxs[(size_t)t * Kpc + kk], fkey(v));
         sc[kk] = -INFINITY;
       }
     }
@@ -475,6 +483,7 @@ __global__ void __launch_bounds__(256) k_union_select(const uint32_t* __restrict
                                                       const int32_t* __restrict__ ncand,
                                                       const int32_t* __restrict__ kfinal,
                                                       const int32_t* __restrict__ best, const int32_t* __restrict__ cnt,
+                                                      const int32_t* __restrict__ maxs, float min_logit, int kmin,
                                                       int Kpc, int Kp, uint32_t* __restrict__ states,
                                                       int32_t* __restrict__ nstates) {
   __shared__ uint32_t key[kMaxCand];
@@ -508,7 +517,20 @@ __global__ void __launch_bounds__(256) k_union_select(const uint32_t* __restrict
       }
       __syncthreads();
     }
-  const int m = min(kfinal[t], nc);
+  int m = min(kfinal[t], nc);
+  if (kmin > 0) {
+    // adaptive size: the candidates some window scores at least min_logit, at
+    // least kmin, at most the target's K
+    __shared__ int n_ok;
+    if (tid == 0) n_ok = 0;
+    __syncthreads();
+    int mine = 0;
+    for (int k = tid; k < nc; k += blockDim.x)
+      if (best[(size_t)t * Kpc + k] < kTopR && fval(maxs[(size_t)t * Kpc + k]) >= min_logit) ++mine;
+    atomicAdd(&n_ok, mine);
+    __syncthreads();
+    m = min(m, max(kmin, n_ok));
+  }
   for (int i = tid; i < m; i += blockDim.x)
     if (key[i] != 0xFFFFFFFFu) sel[key[i] & 0xFFFu] = 1;
   if (tid == 0) base = 0;
@@ -610,16 +632,20 @@ int Context::learned_select_states(int stage, int iteration, int& Kp) {
   if ((e = lw.cnt.ensure((size_t)n * Kpc * 4)) != cudaSuccess) return cuda_fail(e, "learned alloc");
   rc = mlp_forward_device(*this, lw.x.as<__nv_bfloat16>(), (int)rows, lw.score.as<float>(), nullptr, nullptr);
   if (rc != GP_OK) return rc;
+  if ((e = lw.maxs.ensure((size_t)n * Kpc * 4)) != cudaSuccess) return cuda_fail(e, "learned alloc");
+  cudaMemsetAsync(lw.maxs.ptr, 0x80, (size_t)n * Kpc * 4, stream);  // below every score's key
   cudaMemsetAsync(lw.best.ptr, 0x7F, (size_t)n * Kpc * 4, stream);
   cudaMemsetAsync(lw.cnt.ptr, 0, (size_t)n * Kpc * 4, stream);
   k_window_topr<<<dim3(lw.nwin, n), 256, 0, stream>>>(lw.score.as<float>(), lw.ncand.as<int32_t>(), lw.nwin, Kpc,
-                                                       lw.best.as<int32_t>(), lw.cnt.as<int32_t>());
+                                                       lw.best.as<int32_t>(), lw.cnt.as<int32_t>(),
+                                                       lw.maxs.as<int32_t>());
   int kmax = 1;
   for (int i = 0; i < n; ++i) kmax = std::max(kmax, std::min(lw.kfinal[i], host.N));
   Kp = (kmax + 31) / 32 * 32;
   if ((e = w.states.ensure((size_t)n * Kp * 4)) != cudaSuccess) return cuda_fail(e, "alloc states");
   k_union_select<<<n, 256, 0, stream>>>(lw.cand.as<uint32_t>(), lw.ncand.as<int32_t>(), lw.d_kfinal.as<int32_t>(),
-                                        lw.best.as<int32_t>(), lw.cnt.as<int32_t>(), Kpc, Kp,
+                                        lw.best.as<int32_t>(), lw.cnt.as<int32_t>(), lw.maxs.as<int32_t>(),
+                                        lw.min_logit, lw.kmin, Kpc, Kp,
                                         w.states.as<uint32_t>(), w.nstates.as<int32_t>());
   prof.kernel_launches += 2;
   return cudaGetLastError() == cudaSuccess ? GP_OK : cuda_fail(cudaGetLastError(), "learned selection launch");
@@ -730,6 +756,16 @@ int gp_learned_enable(gp_ctx* ctx, int32_t enable, int32_t kcand) {
   c.learned.on = enable != 0;
   c.learned.kcand = kcand;
   return c.learned_apply_k();
+}
+
+int gp_learned_size(gp_ctx* ctx, float min_prob, int32_t kmin) {
+  if (!ctx) return GP_E_ARG;
+  Context& c = *reinterpret_cast<Context*>(ctx);
+  if (kmin < 0 || (kmin > 0 && !(min_prob > 0.f && min_prob < 1.f)))
+    return (c.fail(GP_E_ARG, "learned size: kmin >= 0 and 0 < min_prob < 1"), GP_E_ARG);
+  c.learned.kmin = kmin;
+  c.learned.min_logit = kmin > 0 ? std::log(min_prob / (1.f - min_prob)) : 0.f;
+  return GP_OK;
 }
 
 int32_t gp_learned_windows(gp_ctx* ctx) {

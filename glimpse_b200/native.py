@@ -27,7 +27,7 @@ EXPORTS = [
     "gp_ligate_swap", "gp_gp_accum_get",
     "gp_mlp_param_count", "gp_mlp_init", "gp_mlp_set_params", "gp_mlp_get_params", "gp_mlp_forward",
     "gp_mlp_train_step", "gp_learned_enable", "gp_learned_train", "gp_learned_windows", "gp_state_posteriors",
-    "gp_set_precision", "gp_loglik_get", "gp_tuning_set", "gp_tuning_get",
+    "gp_set_precision", "gp_loglik_get", "gp_tuning_set", "gp_tuning_get", "gp_learned_size",
 ]
 PRECISION_FULL, PRECISION_CKPT_F32, PRECISION_CKPT_BF16 = 0, 1, 2
 
@@ -384,6 +384,10 @@ class Context:
         out = np.zeros(n, np.float64)
         self._check(self.lib.gp_loglik_get(self.h, n, _p(out, C.c_double)))
         return out
+
+    def learned_size(self, min_prob=0.5, kmin=0):
+        """gp_learned_size: kmin = 0 fixed size (the targets' Kpbwt); else adaptive."""
+        self._check(self.lib.gp_learned_size(self.h, C.c_float(min_prob), kmin))
 
     def learned_windows(self):
         n = self.lib.gp_learned_windows(self.h)

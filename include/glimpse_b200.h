@@ -290,6 +290,13 @@ int gp_mlp_train_step(gp_ctx* ctx, int32_t n, const float* x, const float* y, co
  * gp_learned_train); kcand is at most 2048. */
 int gp_learned_enable(gp_ctx* ctx, int32_t enable, int32_t kcand);
 
+/* Size of the learned proposal's conditioning sets. kmin = 0 (the default):
+ * each target's Kpbwt. kmin > 0: the candidates that some window scores at
+ * probability min_prob or more (the network's estimate of y, see
+ * gp_learned_train), at least kmin, at most the target's Kpbwt; the size
+ * then follows how many haplotypes the target's windows need. */
+int gp_learned_size(gp_ctx* ctx, float min_prob, int32_t kmin);
+
 /* Windows of the learned proposal: runs of 256 consecutive common sites; a
  * rare site belongs to the window of the last common site before it. */
 int32_t gp_learned_windows(gp_ctx* ctx);

@@ -130,3 +130,28 @@ def test_autotuned_shapes_do_not_change_results():
     finally:
         for c in ctxs:
             c.close()
+
+
+@pytest.mark.gpu
+def test_adaptive_set_size_stays_in_bounds():
+    """With gp_learned_size(min_prob, kmin) the network sizes each conditioning
+    set: between kmin and the target's K, and fewer states when min_prob rises."""
+    from glimpse_b200 import native
+    w = _workload()
+    P, T = w.panel, w.targets
+    ctx = native.Context(P, kinit=300, kpbwt=200, pbwt_depth=8, pbwt_modulo_cm=0.05)
+    try:
+        ctx.set_targets(T, kpbwt=np.full(T.n, 200, np.int32))
+        ctx.iteration(native.STAGE_INIT, 0)
+        ctx.iteration(native.STAGE_BURN, 1)
+        ctx.learned_train(kcand=512, kpos=8.0, steps=80, batch=4096, lr=1e-3, seed=3)
+        ctx.learned_enable(True, kcand=512)
+        sizes = {}
+        for prob in (0.2, 0.8):
+            ctx.learned_size(prob, 16)
+            ctx.iteration(native.STAGE_BURN, 2)
+            sizes[prob] = np.array([ctx.states(t).size for t in range(T.n)])
+            assert (sizes[prob] >= 16).all() and (sizes[prob] <= 200).all()
+        assert sizes[0.8].sum() <= sizes[0.2].sum()
+    finally:
+        ctx.close()
