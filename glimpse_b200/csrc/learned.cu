@@ -883,7 +883,10 @@ int gp_learned_train(gp_ctx* ctx, int32_t kcand, float kpos, int32_t steps, int3
   // rows with weight: the candidates of windows with polymorphic sites
   const size_t rows = (size_t)c.tw.n * lw.nwin * Kpc;
   std::vector<float> wt(rows);
-  cudaMemcpy(wt.data(), lw.wall.ptr, rows * 4, cudaMemcpyDeviceToHost);
+  // on the context's stream: the labels were written there, and that stream does
+  // not synchronise with the legacy default stream
+  cudaMemcpyAsync(wt.data(), lw.wall.ptr, rows * 4, cudaMemcpyDeviceToHost, c.stream);
+  if ((e = cudaStreamSynchronize(c.stream)) != cudaSuccess) return c.cuda_fail(e, "learned labels");
   std::vector<int64_t> pool;
   pool.reserve(rows);
   for (size_t r = 0; r < rows; ++r)

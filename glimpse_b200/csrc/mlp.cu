@@ -686,7 +686,8 @@ int gp_mlp_forward(gp_ctx* ctx, int32_t n, const float* x, float* score, float* 
   for (int k = 0; k < 2; ++k) {
     float* out = k ? h2 : h1;
     if (!out) continue;
-    cudaMemcpy(hb.data(), (k ? M.h2 : M.h1).ptr, hb.size() * 2, cudaMemcpyDeviceToHost);
+    cudaMemcpyAsync(hb.data(), (k ? M.h2 : M.h1).ptr, hb.size() * 2, cudaMemcpyDeviceToHost, c.stream);
+    if (cudaStreamSynchronize(c.stream) != cudaSuccess) return c.cuda_fail(cudaGetLastError(), "mlp forward");
     for (size_t i = 0; i < hb.size(); ++i) out[i] = __bfloat162float(hb[i]);
   }
   return GP_OK;

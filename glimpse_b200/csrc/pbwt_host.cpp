@@ -597,10 +597,14 @@ int Context::pbwt_states_get(int target, int32_t* counts, int32_t* states, int c
   }
   std::vector<int32_t> cnt((size_t)nh * K);
   std::vector<uint32_t> key((size_t)nh * K * C), id((size_t)nh * K * C);
-  cudaMemcpy(cnt.data(), T.push_cnt.as<int32_t>() + (size_t)h0 * K, cnt.size() * 4, cudaMemcpyDeviceToHost);
-  cudaMemcpy(key.data(), T.push_key.as<uint32_t>() + (size_t)h0 * K * C, key.size() * 4, cudaMemcpyDeviceToHost);
-  cudaError_t e = cudaMemcpy(id.data(), T.push_id.as<uint32_t>() + (size_t)h0 * K * C, id.size() * 4,
-                             cudaMemcpyDeviceToHost);
+  // copies on the context's stream, which the legacy default stream does not wait for
+  cudaMemcpyAsync(cnt.data(), T.push_cnt.as<int32_t>() + (size_t)h0 * K, cnt.size() * 4, cudaMemcpyDeviceToHost,
+                  stream);
+  cudaMemcpyAsync(key.data(), T.push_key.as<uint32_t>() + (size_t)h0 * K * C, key.size() * 4,
+                  cudaMemcpyDeviceToHost, stream);
+  cudaMemcpyAsync(id.data(), T.push_id.as<uint32_t>() + (size_t)h0 * K * C, id.size() * 4, cudaMemcpyDeviceToHost,
+                  stream);
+  cudaError_t e = cudaStreamSynchronize(stream);
   if (e != cudaSuccess) return cuda_fail(e, "pbwt_states_get");
   int w = 0;
   for (int lv = 0; lv < K; ++lv) {
