@@ -120,14 +120,14 @@ struct Context {
   int iteration(int stage, int iteration);
   int finalize();
   int pbwt_prepare_panel();
-  int pbwt_prepare_targets();
+  int pbwt_prepare_targets(bool reset_state);
   int pbwt_select_states(int stage, int iteration, int Kp);
   int pbwt_states_get(int target, int32_t* counts, int32_t* states, int cap);
   int learned_prepare_panel();
   int learned_features(int Kpc, DevBuf& xout);
   int learned_select_states(int stage, int iteration, int& Kp);
   int learned_labels(int Kpc, float kpos, DevBuf& yout, DevBuf& wout);
-  int learned_apply_k();
+  int learned_apply_k(bool reset_state = false);
   int run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_host, int nb, uint8_t* d_h0, uint8_t* d_h1,
                 const uint8_t* d_flat, int iteration, const int32_t* d_target_ids);
 };

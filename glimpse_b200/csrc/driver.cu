@@ -67,7 +67,7 @@ int Context::set_targets(int n, const uint8_t* gl, const uint8_t* flat, const in
   T.finalized = false;
   if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(e, "targets upload");
   learned.kfinal.clear();  // the caller's Kpbwt becomes the learned mode's conditioning-set size
-  return learned_apply_k();
+  return learned_apply_k(true);
 }
 
 // Conditioning sets from states already on the device (impute.states with

@@ -718,7 +718,7 @@ int Context::learned_labels(int Kpc, float kpos, DevBuf& yout, DevBuf& wout) {
 
 // Per-target K arrays for the learned mode: PBWT at the candidate count, the
 // caller's K for the conditioning set.
-int Context::learned_apply_k() {
+int Context::learned_apply_k(bool reset_state) {
   TargetWork& T = tw;
   LearnedWork& lw = learned;
   if (T.n <= 0) return GP_OK;
@@ -734,9 +734,9 @@ int Context::learned_apply_k() {
     if (e != cudaSuccess) return cuda_fail(e, "learned alloc");
     std::vector<int32_t> kf(T.n);
     for (int i = 0; i < T.n; ++i) kf[i] = std::min(lw.kfinal[i], host.N);
-    cudaMemcpy(lw.d_kfinal.ptr, kf.data(), (size_t)T.n * 4, cudaMemcpyHostToDevice);
+    cudaMemcpyAsync(lw.d_kfinal.ptr, kf.data(), (size_t)T.n * 4, cudaMemcpyHostToDevice, stream);
   }
-  return pbwt_prepare_targets();
+  return pbwt_prepare_targets(reset_state);
 }
 
 }  // namespace gp
@@ -872,7 +872,12 @@ int gp_learned_train(gp_ctx* ctx, int32_t kcand, float kpos, int32_t steps, int3
   cudaError_t e = c.impute.states.ensure((size_t)c.tw.n * Kpc * 4);
   if (e == cudaSuccess) e = c.impute.nstates.ensure((size_t)c.tw.n * 4);
   if (e != cudaSuccess) return c.cuda_fail(e, "alloc states");
+  // the sweep advances the targets' PBWT state (tar_hap); training leaves it as it was
+  const size_t nh = c.tw.hap_target.size();
+  if ((e = lw.tarhap_save.ensure(std::max<size_t>(nh, 1))) != cudaSuccess) return c.cuda_fail(e, "learned alloc");
+  cudaMemcpyAsync(lw.tarhap_save.ptr, c.tw.tar_hap.ptr, nh, cudaMemcpyDeviceToDevice, c.stream);
   rc = c.pbwt_select_states(GP_STAGE_BURN, 1 << 20, Kpc);
+  cudaMemcpyAsync(c.tw.tar_hap.ptr, lw.tarhap_save.ptr, nh, cudaMemcpyDeviceToDevice, c.stream);
   if (rc == GP_OK) rc = c.learned_features(Kpc, lw.xall);
   if (rc == GP_OK) rc = c.learned_labels(Kpc, kpos, lw.yall, lw.wall);
   c.learned.on = was_on;

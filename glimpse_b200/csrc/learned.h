@@ -27,12 +27,13 @@ struct LearnedWork {
   DevBuf xall, yall, wall, idx;
   DevBuf urank;                        // [n][N]: PBWT level << 16 | insertion index of every union member
   DevBuf maxs;                         // [n][Kpc]: a candidate's best score over the windows that ranked it
+  DevBuf tarhap_save;                  // the targets' PBWT sweep state, kept across a training sweep
   float min_logit = 0.f;               // adaptive size: keep candidates whose best score reaches this logit
   int kmin = 0;                        // adaptive size: at least this many states (0: fixed size, the caller's K)
   int nwin = 0;
   std::vector<DevBuf*> all() {
     return {&d_kfinal, &planes, &cand, &ncand, &x, &score, &best, &cnt, &site_win, &nsites, &mass0, &mass1,
-            &astore, &aoff, &xall, &yall, &wall, &idx, &urank, &maxs};
+            &astore, &aoff, &xall, &yall, &wall, &idx, &urank, &maxs, &tarhap_save};
   }
 };
 

@@ -401,7 +401,7 @@ int Context::pbwt_prepare_panel() {
 
 // haplotype_set::allocatePBWT (haplotype_set.cpp:229-315): selection groups by
 // rounded cM, halving the modulo for short regions; per-haplotype bookkeeping.
-int Context::pbwt_prepare_targets() {
+int Context::pbwt_prepare_targets(bool reset_state) {
   TargetWork& T = tw;
   const int N = host.N;
   int kglobal = 0;
@@ -429,12 +429,16 @@ int Context::pbwt_prepare_targets() {
   if ((e = T.tar_hap.ensure(nh)) != cudaSuccess) return cuda_fail(e, "alloc");
   std::vector<int32_t> kp(T.n);
   for (int i = 0; i < T.n; ++i) kp[i] = std::min(T.kpbwt_h[i], N);
-  cudaMemcpy(T.d_hap_target.ptr, T.hap_target.data(), nh * 4, cudaMemcpyHostToDevice);
-  cudaMemcpy(T.d_hap_which.ptr, T.hap_which.data(), nh * 4, cudaMemcpyHostToDevice);
-  cudaMemcpy(T.d_target_hap0.ptr, T.target_hap0.data(), T.n * 4, cudaMemcpyHostToDevice);
-  cudaMemcpy(T.d_target_nhap.ptr, T.target_nhap.data(), T.n * 4, cudaMemcpyHostToDevice);
-  cudaMemcpy(T.d_kpbwt.ptr, kp.data(), T.n * 4, cudaMemcpyHostToDevice);
-  cudaMemset(T.tar_hap.ptr, 0, nh);  // tar_hap is zero-initialised once (haplotype_set.cpp:261)
+  // on the context's stream, after any work still in flight there
+  cudaMemcpyAsync(T.d_hap_target.ptr, T.hap_target.data(), nh * 4, cudaMemcpyHostToDevice, stream);
+  cudaMemcpyAsync(T.d_hap_which.ptr, T.hap_which.data(), nh * 4, cudaMemcpyHostToDevice, stream);
+  cudaMemcpyAsync(T.d_target_hap0.ptr, T.target_hap0.data(), T.n * 4, cudaMemcpyHostToDevice, stream);
+  cudaMemcpyAsync(T.d_target_nhap.ptr, T.target_nhap.data(), T.n * 4, cudaMemcpyHostToDevice, stream);
+  cudaMemcpyAsync(T.d_kpbwt.ptr, kp.data(), T.n * 4, cudaMemcpyHostToDevice, stream);
+  // tar_hap is zero-initialised once per target set (haplotype_set.cpp:261) and
+  // then carried across iterations; changing K (the learned proposal) keeps it
+  if (reset_state) cudaMemsetAsync(T.tar_hap.ptr, 0, nh, stream);
+  if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(e, "pbwt targets");
   if (!pbwt_active) return GP_OK;
 
   // modulo and groups
