@@ -241,6 +241,8 @@ def run_ours(args):
     T = w.targets
     kmax = int(T.kpbwt.max())
     ctx = native.Context(w.panel, kinit=w.params["kinit"], kpbwt=kmax, seed=15052011, device=local)
+    ctx.set_precision({"full": native.PRECISION_FULL, "f32": native.PRECISION_CKPT_F32,
+                       "bf16": native.PRECISION_CKPT_BF16}[args.precision])
     ctx.set_targets(T, kpbwt=T.kpbwt)
     stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=torch.device("cuda", local))
 
@@ -305,12 +307,16 @@ def run_ours(args):
     r2 = synth.dosage_r2(ds_h.numpy(), T.truth.sum(1))
 
     peak, peak_kind = load_peaks()
-    achieved = prof["impute_bytes"] / (prof["impute_ms"] / 1000.0) / 1e9 if prof["impute_ms"] > 0 else 0.0
+    # algorithmic bytes per cell: full store 4 B written + 4 B read + 2 x 1/8 B Hvar;
+    # checkpoints 2 x 4/32 (FP32) or 2 x 2/32 (BF16) B + 3 x 1/8 B Hvar (forward, recompute, backward)
+    bpc = {"full": 8.25, "f32": 0.625, "bf16": 0.5}[args.precision]
+    kname = "k_impute_warp" if args.precision == "full" else "k_impute_ckpt"
+    achieved = prof["impute_cells"] * bpc / (prof["impute_ms"] / 1000.0) / 1e9 if prof["impute_ms"] > 0 else 0.0
     per_launch_cells = prof["impute_cells"] / max(1, prof["impute_launches"])
-    tpc = read_traffic("k_impute_warp")
-    roofline = {"bound": "hbm", "kernel": "k_impute_warp (imputation forward-backward)", "achieved": achieved,
+    tpc = read_traffic(kname)
+    roofline = {"bound": "hbm", "kernel": kname + " (imputation forward-backward)", "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                "algorithmic_bytes_per_cell": 8.25, "cells_per_launch": per_launch_cells,
+                "algorithmic_bytes_per_cell": bpc, "cells_per_launch": per_launch_cells,
                 "launch_ms": prof["impute_ms"] / max(1, prof["impute_launches"]),
                 "traffic": (tpc * per_launch_cells) if tpc is not None else None}
     # Phasing (k_phase) is bound by its per-site dependent chain, not by HBM: its
@@ -335,6 +341,10 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "targets_per_gpu": T.n, "iterations_per_step": N_ITER,
                        "l2": "no flush: per-step working set (alpha store, prefix arrays) is tens of GB >> 126 MB L2",
                        "parallelism": f"targets per GPU, {world} rank(s), no collective on the data path"},
+            "precision": {"full": "every forward row in FP32 (as the reference)",
+                          "f32": "FP32 checkpoints every 32 sites, recompute",
+                          "bf16": "BF16 checkpoints every 32 sites, FP32 recompute"}[args.precision],
+            "autotuned": dict(zip(("chains_per_cta", "sweep_haps_per_warp"), ctx.tuning()[:2])),
             "hmm_cells_per_s": world * hmm_cells / (ms / 1000.0),
             "dosage_r2": r2,
             "gpu_launches": int(prof["kernel_launches"]),
@@ -606,6 +616,8 @@ def main():
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--rows", type=int, default=4 << 20)
     ap.add_argument("--groups", type=int, default=2)
+    ap.add_argument("--precision", choices=["full", "f32", "bf16"], default="full",
+                    help="imputation store: every row (default) or FP32 / BF16 checkpoints")
     ap.add_argument("--learned", action="store_true",
                     help="learned proposal vs plain PBWT selection (separate line; see run_learned)")
     ap.add_argument("--learned-frac", type=float, default=0.4)
