@@ -5,6 +5,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <numeric>
 
 #include "context.h"
@@ -101,7 +102,22 @@ Status Context::fail(int code, const std::string& msg) {
 
 int Context::cuda_fail(cudaError_t e, const char* where) {
   err = std::string(where) + ": " + cudaGetErrorString(e);
-  return GP_E_CUDA;
+  return e == cudaErrorMemoryAllocation ? GP_E_NOMEM : GP_E_CUDA;
+}
+
+bool inject_alloc_failure() {
+  static std::mutex mu;
+  static std::string last;
+  static long countdown = 0;
+  const char* v = std::getenv("GLIMPSE_B200_FAIL_ALLOC");
+  std::lock_guard<std::mutex> lk(mu);
+  const std::string cur = v ? v : "";
+  if (cur != last) {
+    last = cur;
+    countdown = cur.empty() ? 0 : std::strtol(cur.c_str(), nullptr, 10);
+  }
+  if (countdown <= 0) return false;
+  return --countdown == 0;
 }
 
 template <class T>

@@ -26,14 +26,17 @@ void unphred_table(float* out) {
 int Context::set_targets(int n, const uint8_t* gl, const uint8_t* flat, const int32_t* ploidy, const int32_t* kp) {
   const int L = panel.L;
   TargetWork& T = tw;
+  // validate before touching the context, so that a refused call leaves it as it was
+  for (int i = 0; i < n; ++i) {
+    if (ploidy[i] != 1 && ploidy[i] != 2) return (fail(GP_E_ARG, "ploidy must be 1 or 2"), GP_E_ARG);
+    if ((kp ? kp[i] : cfg.kpbwt) < 0) return (fail(GP_E_ARG, "negative Kpbwt"), GP_E_ARG);
+  }
   T.n = n;
   T.ploidy_h.assign(ploidy, ploidy + n);
   T.kpbwt_h.resize(n);
   T.diploid.clear();
   for (int i = 0; i < n; ++i) {
-    if (ploidy[i] != 1 && ploidy[i] != 2) return (fail(GP_E_ARG, "ploidy must be 1 or 2"), GP_E_ARG);
     T.kpbwt_h[i] = kp ? kp[i] : cfg.kpbwt;
-    if (T.kpbwt_h[i] < 0) return (fail(GP_E_ARG, "negative Kpbwt"), GP_E_ARG);
     if (ploidy[i] == 2) T.diploid.push_back(i);
   }
   cudaError_t e;

@@ -22,6 +22,12 @@ struct Status {
   std::string msg;
 };
 
+// Host-side fault injection for tests: true when GLIMPSE_B200_FAIL_ALLOC=n is
+// set and this is the n-th buffer growth since it was read (the variable is
+// re-read whenever its value changes). The growth then reports
+// cudaErrorMemoryAllocation without calling cudaMalloc.
+bool inject_alloc_failure();
+
 // Growable device buffer (bytes); contents are not preserved on growth.
 struct DevBuf {
   void* ptr = nullptr;
@@ -31,6 +37,7 @@ struct DevBuf {
     if (ptr) cudaFree(ptr);
     ptr = nullptr;
     cap = 0;
+    if (inject_alloc_failure()) return cudaErrorMemoryAllocation;
     size_t want = bytes + bytes / 8 + 256;
     cudaError_t e = cudaMalloc(&ptr, want);
     if (e == cudaSuccess) cap = want;
