@@ -510,20 +510,44 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   std::vector<int32_t> cnt((size_t)nb * 3);
   cudaMemcpyAsync(cnt.data(), p.counts.ptr, cnt.size() * 4, cudaMemcpyDeviceToHost, stream);
   if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return cuda_fail(e, "phasing vars");
-  std::vector<int64_t> poff(nb), ioff(nb);
-  int64_t ptot = 0, itot = 0;
+  // Blocks in decreasing order of work (VAR sites x state groups), so that the
+  // heaviest targets start first and share an SM with the lightest.
+  std::vector<int32_t> order(nb);
+  std::vector<double> cost(nb);
   int Kmax = 0;
   for (int b = 0; b < nb; ++b) {
     const int t = tsel_host.empty() ? b : tsel_host[b];
+    order[b] = b;
+    cost[b] = (double)cnt[b] * (1.0 + (double)((host_nstates[t] + kPhaseThreads - 1) / kPhaseThreads));
+    Kmax = std::max(Kmax, host_nstates[t]);
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+  // The stored segment-start and flat-het messages, packed per chunk of that
+  // order: chunks run one after another when all entries' stores do not fit
+  // the memory budget together (low coverage makes many flat hets).
+  const size_t budget = store_budget(p.pprob.cap + p.iprob.cap);
+  std::vector<int64_t> poff(nb), ioff(nb);
+  std::vector<int> chunk_start(1, 0);
+  int64_t ptot = 0, itot = 0, pneed = 0, ineed = 0;
+  for (int j = 0; j < nb; ++j) {
+    const int b = order[j];
+    const int t = tsel_host.empty() ? b : tsel_host[b];
     const int K = host_nstates[t];
-    Kmax = std::max(Kmax, K);
+    const int64_t pb = (int64_t)cnt[nb + b] * K * 8, ib = (int64_t)cnt[2 * nb + b] * K * 8;
+    if (j > chunk_start.back() && (size_t)(ptot + pb + itot + ib) * 4 > budget) {
+      chunk_start.push_back(j);
+      ptot = itot = 0;
+    }
     poff[b] = ptot;
     ioff[b] = itot;
-    ptot += (int64_t)cnt[nb + b] * K * 8;
-    itot += (int64_t)cnt[2 * nb + b] * K * 8;
+    ptot += pb;
+    itot += ib;
+    pneed = std::max(pneed, ptot);
+    ineed = std::max(ineed, itot);
   }
-  if ((e = p.pprob.ensure((size_t)std::max<int64_t>(ptot, 1) * 4)) != cudaSuccess) return cuda_fail(e, "alloc pprob");
-  if ((e = p.iprob.ensure((size_t)std::max<int64_t>(itot, 1) * 4)) != cudaSuccess) return cuda_fail(e, "alloc iprob");
+  chunk_start.push_back(nb);
+  if ((e = p.pprob.ensure((size_t)std::max<int64_t>(pneed, 1) * 4)) != cudaSuccess) return cuda_fail(e, "alloc pprob");
+  if ((e = p.iprob.ensure((size_t)std::max<int64_t>(ineed, 1) * 4)) != cudaSuccess) return cuda_fail(e, "alloc iprob");
   if ((e = p.offs.ensure((size_t)nb * 2 * 8)) != cudaSuccess) return cuda_fail(e, "alloc offs");
   if ((e = p.pprob_sum.ensure((size_t)nb * (L + 2) * 8 * 4)) != cudaSuccess) return cuda_fail(e, "alloc psum");
   if ((e = p.pprob_sumsum.ensure((size_t)nb * (L + 2) * 4)) != cudaSuccess) return cuda_fail(e, "alloc pss");
@@ -534,6 +558,8 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   std::vector<int64_t> offs(poff);
   offs.insert(offs.end(), ioff.begin(), ioff.end());
   cudaMemcpyAsync(p.offs.ptr, offs.data(), offs.size() * 8, cudaMemcpyHostToDevice, stream);
+  if ((e = p.order.ensure((size_t)nb * 4)) != cudaSuccess) return cuda_fail(e, "alloc order");
+  cudaMemcpyAsync(p.order.ptr, order.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, stream);
   PhaseStore S;
   S.pprob = p.pprob.as<float>();
   S.pprob_off = p.offs.as<int64_t>();
@@ -545,18 +571,6 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   S.of1 = p.of1.as<float>();
   S.dip = p.dip.as<int32_t>();
   S.err = p.err.as<int32_t>();
-  // Blocks in decreasing order of work (VAR sites x state groups), so that the
-  // heaviest targets start first and share an SM with the lightest.
-  std::vector<int32_t> order(nb);
-  std::vector<double> cost(nb);
-  for (int b = 0; b < nb; ++b) {
-    const int t = tsel_host.empty() ? b : tsel_host[b];
-    order[b] = b;
-    cost[b] = (double)cnt[b] * (1.0 + (double)((host_nstates[t] + kPhaseThreads - 1) / kPhaseThreads));
-  }
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
-  if ((e = p.order.ensure((size_t)nb * 4)) != cudaSuccess) return cuda_fail(e, "alloc order");
-  cudaMemcpyAsync(p.order.ptr, order.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, stream);
   S.order = p.order.as<int32_t>();
   const int J = std::max(1, (Kmax + kPhaseThreads - 1) / kPhaseThreads);
   double pcells = 0;
@@ -564,12 +578,20 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
     const int t = tsel_host.empty() ? b : tsel_host[b];
     pcells += 2.0 * 8.0 * (double)cnt[b] * (double)host_nstates[t];
   }
+  launch_var_records(d_tsel, nb, w.poly.as<int32_t>(), L, panel.cm, mc, V, stream);
   cudaEvent_t ea;
   prof_begin(ea);
-  if (launch_phase(J, d_tsel, nb, w.nstates.as<int32_t>(), w.hvar.as<uint32_t>(), w.WB, w.Kp, w.poly.as<int32_t>(),
-                   w.npoly.as<int32_t>(), L, panel.cm, V, S, mc, cfg.seed, iteration, d_target_ids, stream) != GP_OK)
-    return (fail(GP_E_ARG, "phasing: too many states"), GP_E_ARG);
+  for (size_t c = 0; c + 1 < chunk_start.size(); ++c) {
+    PhaseStore Sc = S;
+    Sc.order = S.order + chunk_start[c];
+    if (launch_phase(J, d_tsel, chunk_start[c + 1] - chunk_start[c], w.nstates.as<int32_t>(), w.hvar.as<uint32_t>(),
+                     w.WB, w.Kp, w.poly.as<int32_t>(), w.npoly.as<int32_t>(), L, panel.cm, V, Sc, mc, cfg.seed,
+                     iteration, d_target_ids, stream) != GP_OK)
+      return (fail(GP_E_ARG, "phasing: too many states"), GP_E_ARG);
+    prof.kernel_launches += 1;
+  }
   prof_end(ea, 1, pcells);
+  phase_chunks = (int)chunk_start.size() - 1;
   // SAMPLE_DIP's invalid-sum flags (the reference asserts there, phasing_hmm.cpp:175).
   if (phase_err_cap < nb) {
     if (phase_err_host) cudaFreeHost(phase_err_host);
@@ -584,7 +606,7 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   for (int b = 0; b < nb; ++b) phase_err_ids[b] = tsel_host.empty() ? b : tsel_host[b];
   launch_phase_writeback(d_tsel, nb, w.poly.as<int32_t>(), w.polyidx.as<int32_t>(), L, V, S, mc, cfg.seed, iteration,
                          d_target_ids, d_h0, d_h1, stream);
-  prof.kernel_launches += 4;
+  prof.kernel_launches += 3;  // VAR records and the two write-back kernels (k_phase counted per chunk)
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "phasing launch");
   last_phase_nseg.assign(cnt.begin() + nb, cnt.begin() + 2 * nb);
   return GP_OK;

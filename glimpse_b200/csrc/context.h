@@ -108,6 +108,7 @@ struct Context {
   DevBuf ckpt, ckpt_sum, ckpt_scratch, loglik;  // checkpointed imputation (kernels_impute_ckpt.cu)
   int loglik_n = 0;                             // entries of the last checkpointed imputation call
   int impute_chunks = 0;  // launches pairs of the last run_impute (1 when the whole batch fit)
+  int phase_chunks = 0;   // k_phase launches of the last run_phase
   // Autotuner: launch shapes picked by timing every candidate on the first batch
   // large enough to tell them apart; fixed_* (gp_tuning_set) override it.
   int tune_cpc = 0, tune_hpw = 0;     // chosen chains per CTA / haplotypes per sweep warp (0: not yet)

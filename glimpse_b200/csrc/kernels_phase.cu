@@ -720,10 +720,15 @@ void launch_build_vars(const int32_t* tsel, int nb, const int32_t* poly, const i
   k_build_vars<512, 8><<<nb, 512, 0, s>>>(poly, npoly, h0, h1, flat, lq, L, tsel, V);
 }
 
+void launch_var_records(const int32_t* tsel, int nb, const int32_t* poly, int L, const double* cm,
+                        const ModelConst& mc, PhaseVars V, cudaStream_t s) {
+  k_var_records<<<dim3(32, nb), 256, 0, s>>>(tsel, poly, L, cm, mc, V);
+}
+
 int launch_phase(int J, const int32_t* tsel, int nb, const int32_t* nstates, const uint32_t* hvar, int WB, int Kp,
                  const int32_t* poly, const int32_t* npoly, int L, const double* cm, PhaseVars V, PhaseStore S,
                  const ModelConst& mc, uint64_t seed, int iteration, const int32_t* target_ids, cudaStream_t s) {
-  k_var_records<<<dim3(32, nb), 256, 0, s>>>(tsel, poly, L, cm, mc, V);
+  (void)cm;
   switch (J) {
     case 1: k_phase<1><<<nb, PT, 0, s>>>(tsel, nstates, npoly, hvar, WB, Kp, L, V, S, mc, seed, iteration, target_ids); break;
     case 2: k_phase<2><<<nb, PT, 0, s>>>(tsel, nstates, npoly, hvar, WB, Kp, L, V, S, mc, seed, iteration, target_ids); break;

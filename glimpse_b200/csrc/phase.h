@@ -47,6 +47,11 @@ struct PhaseStore {
 void launch_build_vars(const int32_t* tsel, int nb, const int32_t* poly, const int32_t* npoly, const uint8_t* h0,
                        const uint8_t* h1, const uint8_t* flat, const uint8_t* lq, int L, PhaseVars V,
                        cudaStream_t s);
+// Per-VAR transition records of all nb entries (before the phasing launches).
+void launch_var_records(const int32_t* tsel, int nb, const int32_t* poly, int L, const double* cm,
+                        const ModelConst& mc, PhaseVars V, cudaStream_t s);
+// k_phase over nb blocks: block i runs entry S.order[i] (S.order may point into
+// a longer order, for a chunk of the batch).
 int launch_phase(int J, const int32_t* tsel, int nb, const int32_t* nstates, const uint32_t* hvar, int WB, int Kp,
                  const int32_t* poly, const int32_t* npoly, int L, const double* cm, PhaseVars V, PhaseStore S,
                  const ModelConst& mc, uint64_t seed, int iteration, const int32_t* target_ids, cudaStream_t s);

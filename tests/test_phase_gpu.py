@@ -72,3 +72,31 @@ def test_invalid_diplotype_sums_return_data_error(small_workload):
     finally:
         good.close()
         bad.close()
+
+
+@pytest.mark.gpu
+def test_chunked_phasing_matches_single_launch(small_workload, monkeypatch):
+    """When the targets' stored phasing messages do not fit the device-memory
+    budget together, k_phase runs in consecutive chunks of the batch
+    (GLIMPSE_B200_STORE_BUDGET_MB lowers the budget so that a small batch takes
+    that path). The rephased haplotypes must be identical."""
+    from glimpse_b200 import native
+    w = small_workload
+    P, T = w.panel, w.targets
+    rng = np.random.default_rng(9)
+    cases = []
+    for i in range(9):
+        t = i % T.n
+        s = np.sort(rng.choice(P.n_ref_haps, size=int(rng.integers(50, 520)), replace=False)).astype(np.uint32)
+        cases.append((s, _noisy_haps(rng, T.truth[t, 0]), _noisy_haps(rng, T.truth[t, 1]), T.flat[t], t))
+    args = ([c[0] for c in cases], np.stack([c[1] for c in cases]), np.stack([c[2] for c in cases]),
+            np.stack([c[3] for c in cases]), 4)
+    ctx = native.Context(P)
+    try:
+        a0, a1 = ctx.rephase_batch(*args, target_ids=[c[4] for c in cases])
+        monkeypatch.setenv("GLIMPSE_B200_STORE_BUDGET_MB", "1")
+        b0, b1 = ctx.rephase_batch(*args, target_ids=[c[4] for c in cases])
+        monkeypatch.delenv("GLIMPSE_B200_STORE_BUDGET_MB")
+        assert np.array_equal(a0, b0) and np.array_equal(a1, b1)
+    finally:
+        ctx.close()
