@@ -312,15 +312,23 @@ int Context::build_condsets(int n, const std::vector<int64_t>& off, const std::v
   return GP_OK;
 }
 
-// Bytes the forward-backward store may take: half of the device's memory, and
-// no more than is free now (plus what the store already holds) less 8 GiB for
-// the rest of the iteration. GLIMPSE_B200_STORE_BUDGET_MB lowers it (tests use
-// it to run the chunked path on small batches).
-size_t Context::store_budget(size_t held) {
-  size_t fr = 0, tot = 0;
-  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return held;
-  const size_t reserve = size_t(8) << 30;
-  size_t b = std::min(tot / 2, fr + held > reserve ? fr + held - reserve : held);
+// Bytes a growable store may take when `need` bytes are wanted and `held`
+// are already allocated: everything wanted when it fits what is held (no query
+// of the device), else half of the device's memory and no more than is free
+// now (plus what the store holds) less 8 GiB for the rest of the iteration.
+// GLIMPSE_B200_STORE_BUDGET_MB lowers it (tests use it to run the chunked
+// paths on small batches).
+size_t Context::store_budget(size_t held, size_t need) {
+  size_t b = need;
+  if (need > held) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+      const size_t reserve = size_t(8) << 30;
+      b = std::min(tot / 2, fr + held > reserve ? fr + held - reserve : held);
+    } else {
+      b = held;
+    }
+  }
   if (const char* env = std::getenv("GLIMPSE_B200_STORE_BUDGET_MB")) {
     const long long mb = std::atoll(env);
     if (mb > 0) b = std::min(b, (size_t)mb << 20);
@@ -349,7 +357,9 @@ int Context::run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
   for (int i = 0; i < n; ++i) order[i] = i;
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return impute_np[x] > impute_np[y]; });
   // chunks of the order whose stores fit the budget
-  const size_t budget = store_budget(w.alpha.cap);
+  size_t need_all = 0;
+  for (int i = 0; i < n; ++i) need_all += (size_t)impute_np[i] * w.Ks * 4;
+  const size_t budget = store_budget(w.alpha.cap, need_all);
   std::vector<int64_t> aoff(n);
   std::vector<int32_t> split(n);
   std::vector<int> chunk_start(1, 0);
@@ -525,7 +535,15 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   // The stored segment-start and flat-het messages, packed per chunk of that
   // order: chunks run one after another when all entries' stores do not fit
   // the memory budget together (low coverage makes many flat hets).
-  const size_t budget = store_budget(p.pprob.cap + p.iprob.cap);
+  size_t need_p = 0, need_i = 0;
+  for (int b = 0; b < nb; ++b) {
+    const int K = host_nstates[tsel_host.empty() ? b : tsel_host[b]];
+    need_p += (size_t)cnt[nb + b] * K * 8 * 4;
+    need_i += (size_t)cnt[2 * nb + b] * K * 8 * 4;
+  }
+  // both stores already large enough: the whole batch fits without asking the device
+  const bool fits = need_p <= p.pprob.cap && need_i <= p.iprob.cap;
+  const size_t budget = store_budget(fits ? need_p + need_i : p.pprob.cap + p.iprob.cap, need_p + need_i);
   std::vector<int64_t> poff(nb), ioff(nb);
   std::vector<int> chunk_start(1, 0);
   int64_t ptot = 0, itot = 0, pneed = 0, ineed = 0;

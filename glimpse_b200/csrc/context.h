@@ -102,7 +102,7 @@ struct Context {
   int create_panel(const gp_panel_desc& d);
   int build_condsets(int n, const std::vector<int64_t>& off, const std::vector<uint32_t>& states);
   int run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp);
-  size_t store_budget(size_t held);
+  size_t store_budget(size_t held, size_t need);
   int run_impute_ckpt(const float* d_hl, const uint8_t* d_flat, float* d_hp);
   int precision_mode = GP_PRECISION_FULL;
   DevBuf ckpt, ckpt_sum, ckpt_scratch, loglik;  // checkpointed imputation (kernels_impute_ckpt.cu)

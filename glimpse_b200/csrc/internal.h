@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -21,6 +23,21 @@ struct Status {
   int code = GP_OK;
   std::string msg;
 };
+
+// A kernel's dynamic shared-memory limit, set once per device (the attribute is
+// per device; contexts may sit on different devices). F is the kernel.
+template <auto F>
+cudaError_t set_smem_limit_once(int bytes) {
+  static std::atomic<uint64_t> done{0};  // bit d: set on device d
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const uint64_t bit = 1ull << (dev & 63);
+  if (dev < 64 && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+  e = cudaFuncSetAttribute(F, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess && dev < 64) done.fetch_or(bit, std::memory_order_acq_rel);
+  return e;
+}
 
 // Host-side fault injection for tests: true when GLIMPSE_B200_FAIL_ALLOC=n is
 // set and this is the n-th buffer growth since it was read (the variable is

@@ -506,10 +506,7 @@ static int launch_chains(const ChainArgs& a, int cpc, cudaStream_t s) {
   if (cpc < 1 || cpc > kMaxChainsPerCta) return GP_E_ARG;
   const size_t sm = impute_warp_smem(J, cpc);
   if (sm > 200 * 1024) return GP_E_ARG;
-  // The attribute is per device (contexts may sit on different devices);
-  // setting it at every launch is cheap.
-  if (cudaFuncSetAttribute(k_impute_warp<J, W, POST>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) !=
-      cudaSuccess)
+  if (set_smem_limit_once<k_impute_warp<J, W, POST>>(200 * 1024) != cudaSuccess)
     return GP_E_CUDA;
   const dim3 g((a.nchains + cpc - 1) / cpc);
   k_impute_warp<J, W, POST><<<g, 32 * W * cpc, sm, s>>>(a);

@@ -490,8 +490,7 @@ static size_t sweep_smem(const PbwtSelectArgs& a, int& D) {
 void launch_pbwt_sweep(const PbwtSelectArgs& a, int hpw, cudaStream_t s) {
   int D = 0;
   const size_t smem = sweep_smem(a, D);
-  // The attribute is per device; setting it at every launch is cheap.
-  if (smem > (48u << 10)) cudaFuncSetAttribute(k_pbwt_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 << 10);
+  if (smem > (48u << 10)) set_smem_limit_once<k_pbwt_sweep>(200 << 10);
   k_pbwt_sweep<<<(a.n_haps + hpw - 1) / hpw, 32, smem, s>>>(a, D, hpw);
 }
 

@@ -408,7 +408,7 @@ cudaError_t launch_mlp_fwd(const MlpFwdArgs& a, int grid, cudaStream_t s) {
   if (a.n <= 0) return cudaSuccess;
   const int ntiles = (a.n + kTileM - 1) / kTileM;
   grid = std::max(1, std::min(grid, ntiles));
-  cudaError_t e = cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemFwd);
+  cudaError_t e = set_smem_limit_once<k_mlp_fwd>((int)kSmemFwd);
   if (e != cudaSuccess) return e;
   k_mlp_fwd<<<grid, kFwdThreads, kSmemFwd, s>>>(a);
   return cudaGetLastError();
@@ -417,7 +417,7 @@ cudaError_t launch_mlp_fwd(const MlpFwdArgs& a, int grid, cudaStream_t s) {
 template <int NT, int EPI>
 static cudaError_t gemm_launch(const GemmArgs& g, int splits, cudaStream_t s) {
   constexpr size_t smem = 2 * (kTileM * 64 * 2 + NT * 64 * 2) + 64;
-  cudaError_t e = cudaFuncSetAttribute(k_gemm_tn<NT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = set_smem_limit_once<k_gemm_tn<NT, EPI>>((int)smem);
   if (e != cudaSuccess) return e;
   const dim3 grid((g.M + kTileM - 1) / kTileM, (g.N + NT - 1) / NT, splits);
   k_gemm_tn<NT, EPI><<<grid, 128, smem, s>>>(g);
