@@ -45,29 +45,33 @@ struct CkptArgs {
 };
 
 // Sums of N values over the CTA: warp butterflies, then the warps in one tree.
+// The partials alternate between two buffers, so one barrier per reduction
+// suffices: a reduction's writes go to the buffer that the previous one did
+// not read, and the one before that was read before the previous barrier.
 template <int N>
-__device__ __forceinline__ void cta_sum(float (&v)[N], float (*red)[kCW]) {
+__device__ __forceinline__ void cta_sum(float (&v)[N], float (*red)[3][kCW], int& buf) {
 #pragma unroll
   for (int i = 0; i < N; ++i)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v[i] = __fadd_rn(v[i], __shfl_xor_sync(0xFFFFFFFFu, v[i], o));
-  __syncthreads();  // the previous reduction's reads of red are done
   if ((threadIdx.x & 31) == 0)
 #pragma unroll
-    for (int i = 0; i < N; ++i) red[i][threadIdx.x >> 5] = v[i];
+    for (int i = 0; i < N; ++i) red[buf][i][threadIdx.x >> 5] = v[i];
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < N; ++i) {
-    const float* r = red[i];
+    const float* r = red[buf][i];
     v[i] = __fadd_rn(__fadd_rn(__fadd_rn(r[0], r[1]), __fadd_rn(r[2], r[3])),
                      __fadd_rn(__fadd_rn(r[4], r[5]), __fadd_rn(r[6], r[7])));
   }
+  buf ^= 1;
 }
 
 template <bool BF16>
 __global__ void __launch_bounds__(kCT) k_impute_ckpt(CkptArgs a) {
   static_assert(kCW == 8, "eight warps");
-  __shared__ float red[3][kCW];
+  __shared__ float red[2][3][kCW];
+  int buf = 0;
   const int t = blockIdx.x, tid = threadIdx.x;
   const int np = a.npoly[t], K = a.nstates[t];
   if (np <= 0 || K <= 0) return;
@@ -130,7 +134,7 @@ __global__ void __launch_bounds__(kCT) k_impute_ckpt(CkptArgs a) {
       x[j] = valid[j] ? __fmul_rn(pc, (w[j] & m) ? ey : ex) : 0.f;
       s[0] = __fadd_rn(s[0], x[j]);
     }
-    cta_sum<1>(s, red);
+    cta_sum<1>(s, red, buf);
     acc = (l == 0 && f) ? 1.0f : s[0];  // AlphaSum = 1 at a flat first site (imputation_hmm.cpp:156)
   };
 
@@ -200,7 +204,7 @@ __global__ void __launch_bounds__(kCT) k_impute_ckpt(CkptArgs a) {
         xb[j] = __fmul_rn(pc, bit ? ey : ex);
         v[0] = __fadd_rn(v[0], xb[j]);
       }
-      cta_sum<3>(v, red);
+      cta_sum<3>(v, red, buf);
       bacc = (last && f) ? 1.0f : v[0];  // betaSum = 1 at a flat last site (imputation_hmm.cpp:285)
       if (tid == 0) *reinterpret_cast<float2*>(HP + 2 * PL[l]) = make_float2(v[1], v[2]);
     }
