@@ -532,40 +532,8 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
     Kmax = std::max(Kmax, host_nstates[t]);
   }
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
-  // The stored segment-start and flat-het messages, packed per chunk of that
-  // order: chunks run one after another when all entries' stores do not fit
-  // the memory budget together (low coverage makes many flat hets).
-  size_t need_p = 0, need_i = 0;
-  for (int b = 0; b < nb; ++b) {
-    const int K = host_nstates[tsel_host.empty() ? b : tsel_host[b]];
-    need_p += (size_t)cnt[nb + b] * K * 8 * 4;
-    need_i += (size_t)cnt[2 * nb + b] * K * 8 * 4;
-  }
-  // both stores already large enough: the whole batch fits without asking the device
-  const bool fits = need_p <= p.pprob.cap && need_i <= p.iprob.cap;
-  const size_t budget = store_budget(fits ? need_p + need_i : p.pprob.cap + p.iprob.cap, need_p + need_i);
-  std::vector<int64_t> poff(nb), ioff(nb);
-  std::vector<int> chunk_start(1, 0);
-  int64_t ptot = 0, itot = 0, pneed = 0, ineed = 0;
-  for (int j = 0; j < nb; ++j) {
-    const int b = order[j];
-    const int t = tsel_host.empty() ? b : tsel_host[b];
-    const int K = host_nstates[t];
-    const int64_t pb = (int64_t)cnt[nb + b] * K * 8, ib = (int64_t)cnt[2 * nb + b] * K * 8;
-    if (j > chunk_start.back() && (size_t)(ptot + pb + itot + ib) * 4 > budget) {
-      chunk_start.push_back(j);
-      ptot = itot = 0;
-    }
-    poff[b] = ptot;
-    ioff[b] = itot;
-    ptot += pb;
-    itot += ib;
-    pneed = std::max(pneed, ptot);
-    ineed = std::max(ineed, itot);
-  }
-  chunk_start.push_back(nb);
-  if ((e = p.pprob.ensure((size_t)std::max<int64_t>(pneed, 1) * 4)) != cudaSuccess) return cuda_fail(e, "alloc pprob");
-  if ((e = p.iprob.ensure((size_t)std::max<int64_t>(ineed, 1) * 4)) != cudaSuccess) return cuda_fail(e, "alloc iprob");
+  // The per-entry buffers of fixed size come first, so that the budget below
+  // sees the memory they leave.
   if ((e = p.offs.ensure((size_t)nb * 2 * 8)) != cudaSuccess) return cuda_fail(e, "alloc offs");
   if ((e = p.pprob_sum.ensure((size_t)nb * (L + 2) * 8 * 4)) != cudaSuccess) return cuda_fail(e, "alloc psum");
   if ((e = p.pprob_sumsum.ensure((size_t)nb * (L + 2) * 4)) != cudaSuccess) return cuda_fail(e, "alloc pss");
@@ -573,17 +541,46 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   if ((e = p.of1.ensure((size_t)nb * L * 8 * 4)) != cudaSuccess) return cuda_fail(e, "alloc of1");
   if ((e = p.dip.ensure((size_t)nb * (L + 2) * 4)) != cudaSuccess) return cuda_fail(e, "alloc dip");
   if ((e = p.err.ensure((size_t)nb * 4)) != cudaSuccess) return cuda_fail(e, "alloc err");
+  if ((e = p.order.ensure((size_t)nb * 4)) != cudaSuccess) return cuda_fail(e, "alloc order");
+  // The stored segment-start and flat-het messages of every entry, its two
+  // regions side by side in one pool, packed per chunk of that order: chunks
+  // run one after another when all entries' stores do not fit the memory
+  // budget together (low coverage makes many flat hets).
+  size_t need_all = 0;
+  for (int b = 0; b < nb; ++b) {
+    const int K = host_nstates[tsel_host.empty() ? b : tsel_host[b]];
+    need_all += ((size_t)cnt[nb + b] + (size_t)cnt[2 * nb + b]) * K * 8 * 4;
+  }
+  const size_t budget = store_budget(p.pool.cap, need_all);
+  std::vector<int64_t> poff(nb), ioff(nb);
+  std::vector<int> chunk_start(1, 0);
+  int64_t tot = 0, need = 0;
+  for (int j = 0; j < nb; ++j) {
+    const int b = order[j];
+    const int t = tsel_host.empty() ? b : tsel_host[b];
+    const int K = host_nstates[t];
+    const int64_t pb = (int64_t)cnt[nb + b] * K * 8, ib = (int64_t)cnt[2 * nb + b] * K * 8;
+    if (j > chunk_start.back() && (size_t)(tot + pb + ib) * 4 > budget) {
+      chunk_start.push_back(j);
+      tot = 0;
+    }
+    poff[b] = tot;
+    ioff[b] = tot + pb;
+    tot += pb + ib;
+    need = std::max(need, tot);
+  }
+  chunk_start.push_back(nb);
+  if ((e = p.pool.ensure((size_t)std::max<int64_t>(need, 1) * 4)) != cudaSuccess) return cuda_fail(e, "alloc phasing store");
   std::vector<int64_t> offs(poff);
   offs.insert(offs.end(), ioff.begin(), ioff.end());
   cudaMemcpyAsync(p.offs.ptr, offs.data(), offs.size() * 8, cudaMemcpyHostToDevice, stream);
-  if ((e = p.order.ensure((size_t)nb * 4)) != cudaSuccess) return cuda_fail(e, "alloc order");
   cudaMemcpyAsync(p.order.ptr, order.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, stream);
   PhaseStore S;
-  S.pprob = p.pprob.as<float>();
+  S.pprob = p.pool.as<float>();
   S.pprob_off = p.offs.as<int64_t>();
   S.pprob_sum = p.pprob_sum.as<float>();
   S.pprob_sumsum = p.pprob_sumsum.as<float>();
-  S.iprob = p.iprob.as<float>();
+  S.iprob = p.pool.as<float>();
   S.iprob_off = p.offs.as<int64_t>() + nb;
   S.iprob_sum = p.iprob_sum.as<float>();
   S.of1 = p.of1.as<float>();

@@ -101,9 +101,10 @@ struct ImputeWork {
 // Scratch of the phasing HMM.
 struct PhaseWork {
   DevBuf rel, code, seg, miss, seg_start, counts, ytp, ytn, vflags, recb, recf;
-  DevBuf pprob, iprob, offs, pprob_sum, pprob_sumsum, iprob_sum, of1, dip, err, order;
+  DevBuf pool;  // the stored segment-start and flat-het messages of one chunk of entries
+  DevBuf offs, pprob_sum, pprob_sumsum, iprob_sum, of1, dip, err, order;
   std::vector<DevBuf*> all() {
-    return {&rel, &code, &seg, &miss, &seg_start, &counts, &ytp, &ytn, &vflags, &recb, &recf, &pprob, &iprob, &offs,
+    return {&rel, &code, &seg, &miss, &seg_start, &counts, &ytp, &ytn, &vflags, &recb, &recf, &pool, &offs,
             &pprob_sum, &pprob_sumsum, &iprob_sum, &of1, &dip, &err, &order};
   }
 };
