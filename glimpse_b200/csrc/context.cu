@@ -258,6 +258,7 @@ Context::~Context() {
   lig_a.release(); lig_b.release(); lig_s.release(); lig_cnt.release();
   for (DevBuf* b : mlp.all()) b->release();
   tune_tarhap.release();
+  list_off.release(); list_ids.release(); merged_states.release();
   ckpt.release(); ckpt_sum.release(); ckpt_scratch.release(); loglik.release();
   for (DevBuf* b : learned.all()) b->release();
   if (phase_err_host) cudaFreeHost(phase_err_host);
@@ -650,6 +651,8 @@ void gp_config_defaults(gp_config* c) {
 int gp_ctx_create(const gp_panel_desc* panel, const gp_config* cfg, gp_ctx** out) {
   if (!panel || !cfg || !out) return GP_E_ARG;
   *out = nullptr;
+  // caller_parameters.cpp:255-258: Kinit and Kpbwt non-negative
+  if (cfg->kinit < 0 || cfg->kpbwt < 0) return GP_E_ARG;
   int dev_count = 0;
   if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count <= cfg->device) return GP_E_CUDA;
   if (cudaSetDevice(cfg->device) != cudaSuccess) return GP_E_CUDA;

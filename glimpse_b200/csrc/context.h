@@ -115,9 +115,15 @@ struct Context {
   int fixed_cpc = 0, fixed_hpw = 0;
   float tune_ms[7] = {0, 0, 0, 0, 0, 0, 0};  // phase-1 ms for 1, 2, 4 chains per CTA; sweep ms for 1, 2, 4, 8
   DevBuf tune_tarhap;
+  // --state-list: per target the sorted union of its haplotypes' rows (empty: no lists)
+  std::vector<int32_t> list_len;
+  DevBuf list_off, list_ids, merged_states;
+  int set_state_lists(int n_haps, const int64_t* off, const int32_t* ids);
+  int merge_state_lists(int& Kp);
   int set_targets(int n, const uint8_t* gl, const uint8_t* flat, const int32_t* ploidy, const int32_t* kp);
   int build_condsets_device(int n, int Kp);
   int select_states(int stage, int iteration, int& Kp);
+  int init_select_states(int iteration, int Kp, int kinit);
   int iteration(int stage, int iteration);
   int finalize();
   int pbwt_prepare_panel();

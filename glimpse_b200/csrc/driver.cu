@@ -32,6 +32,7 @@ int Context::set_targets(int n, const uint8_t* gl, const uint8_t* flat, const in
     if ((kp ? kp[i] : cfg.kpbwt) < 0) return (fail(GP_E_ARG, "negative Kpbwt"), GP_E_ARG);
   }
   T.n = n;
+  list_len.clear();  // state lists belong to a target set
   T.ploidy_h.assign(ploidy, ploidy + n);
   T.kpbwt_h.resize(n);
   T.diploid.clear();
@@ -104,16 +105,23 @@ int Context::build_condsets_device(int n, int Kp) {
 }
 
 // Stage selection into impute.states / impute.nstates. Returns the stride Kp.
+// The branches of conditioning_set::compactSelection (conditioning_set.cpp:82-121):
+// the init selection at the init stage when Kinit > 0; the whole panel when
+// Kpbwt >= n_ref_haps; else the PBWT (or learned) selection, which at the init
+// stage (Kinit = 0) or with Kpbwt = 0 is empty. The state lists then join every
+// set but the whole panel's.
 int Context::select_states(int stage, int iteration, int& Kp) {
   TargetWork& T = tw;
   ImputeWork& w = impute;
   const int n = T.n;
   const int N = panel.N;
   const int kinit = std::min(cfg.kinit, N);
+  const bool lists = !list_len.empty();
   cudaError_t e;
   int Kmax = 0;
   bool full_panel = false;
-  if (stage == GP_STAGE_INIT && kinit > 0) {
+  const bool init_sel = stage == GP_STAGE_INIT && kinit > 0;
+  if (init_sel) {
     Kmax = kinit;
   } else {
     for (int i = 0; i < n; ++i) {
@@ -123,43 +131,62 @@ int Context::select_states(int stage, int iteration, int& Kp) {
     }
     if (full_panel) Kmax = N;
   }
-  if (Kmax <= 0) return (fail(GP_E_ARG, "Kinit/Kpbwt of zero needs a state list (not supported)"), GP_E_ARG);
+  // no selection: the init stage without Kinit, or Kpbwt = 0 for every target
+  const bool empty_sel = !init_sel && !full_panel && (stage == GP_STAGE_INIT || !pbwt_active);
+  if (empty_sel) Kmax = 0;
+  if (Kmax <= 0 && !lists)
+    return (fail(GP_E_ARG, "Kinit/Kpbwt of zero needs a state list (gp_state_lists_set)"), GP_E_ARG);
   if (Kmax > kMaxStates)
     return (fail(GP_E_ARG, "more than " + std::to_string(kMaxStates) + " conditioning states per target"), GP_E_ARG);
-  Kp = (Kmax + 31) / 32 * 32;
+  Kp = std::max(32, (Kmax + 31) / 32 * 32);
   if ((e = w.states.ensure((size_t)n * Kp * 4)) != cudaSuccess) return cuda_fail(e, "alloc states");
   if ((e = w.nstates.ensure((size_t)n * 4)) != cudaSuccess) return cuda_fail(e, "alloc nstates");
-  if (stage == GP_STAGE_INIT && kinit > 0) {
-    InitSelArgs a;
-    a.gl = T.gl.as<uint8_t>();
-    a.flat = T.flat.as<uint8_t>();
-    a.ploidy = T.ploidy.as<int32_t>();
-    a.common = panel.common;
-    a.lq = panel.lq;
-    a.major = panel.major;
-    a.cref = panel.cref;
-    a.calt = panel.calt;
-    a.svar_off = panel.svar_off;
-    a.svar_haps = panel.svar_haps;
-    a.sind = T.sind.as<int32_t>();
-    a.nsind = T.nsind.as<int32_t>();
-    a.bitmap = T.bitmap.as<uint32_t>();
-    a.states = w.states.as<uint32_t>();
-    a.nstates = w.nstates.as<int32_t>();
-    a.n = n;
-    a.L = panel.L;
-    a.N = N;
-    a.Kp = Kp;
-    a.kinit = kinit;
-    a.max_mac = host.max_rare_mac;
-    a.seed = cfg.seed;
-    a.iteration = iteration;
-    launch_init_select(a, stream);
-    prof.kernel_launches += 2;
-    return GP_OK;
+  int rc = GP_OK;
+  if (empty_sel) {
+    cudaMemsetAsync(w.nstates.ptr, 0, (size_t)n * 4, stream);
+  } else if (init_sel) {
+    rc = init_select_states(iteration, Kp, kinit);
+  } else if (learned.on && mlp.ready) {
+    rc = learned_select_states(stage, iteration, Kp);
+  } else {
+    rc = pbwt_select_states(stage, iteration, Kp);
   }
-  if (learned.on && mlp.ready) return learned_select_states(stage, iteration, Kp);
-  return pbwt_select_states(stage, iteration, Kp);
+  if (rc != GP_OK || !lists || full_panel) return rc;
+  return merge_state_lists(Kp);
+}
+
+// Init-stage selection (haplotype_set.cpp:775-833) for every target.
+int Context::init_select_states(int iteration, int Kp, int kinit) {
+  TargetWork& T = tw;
+  ImputeWork& w = impute;
+  const int n = T.n;
+  InitSelArgs a;
+  a.gl = T.gl.as<uint8_t>();
+  a.flat = T.flat.as<uint8_t>();
+  a.ploidy = T.ploidy.as<int32_t>();
+  a.common = panel.common;
+  a.lq = panel.lq;
+  a.major = panel.major;
+  a.cref = panel.cref;
+  a.calt = panel.calt;
+  a.svar_off = panel.svar_off;
+  a.svar_haps = panel.svar_haps;
+  a.sind = T.sind.as<int32_t>();
+  a.nsind = T.nsind.as<int32_t>();
+  a.bitmap = T.bitmap.as<uint32_t>();
+  a.states = w.states.as<uint32_t>();
+  a.nstates = w.nstates.as<int32_t>();
+  a.n = n;
+  a.L = panel.L;
+  a.N = panel.N;
+  a.Kp = Kp;
+  a.kinit = kinit;
+  a.max_mac = host.max_rare_mac;
+  a.seed = cfg.seed;
+  a.iteration = iteration;
+  launch_init_select(a, stream);
+  prof.kernel_launches += 2;
+  return GP_OK;
 }
 
 int Context::iteration(int stage, int iteration) {

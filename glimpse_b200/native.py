@@ -28,6 +28,7 @@ EXPORTS = [
     "gp_mlp_param_count", "gp_mlp_init", "gp_mlp_set_params", "gp_mlp_get_params", "gp_mlp_forward",
     "gp_mlp_train_step", "gp_learned_enable", "gp_learned_train", "gp_learned_windows", "gp_state_posteriors",
     "gp_set_precision", "gp_loglik_get", "gp_tuning_set", "gp_tuning_get", "gp_learned_size",
+    "gp_state_lists_set",
 ]
 PRECISION_FULL, PRECISION_CKPT_F32, PRECISION_CKPT_BF16 = 0, 1, 2
 
@@ -267,6 +268,17 @@ class Context:
             self._tk["kp"] = kp
         self._check(self.lib.gp_targets_set(self.h, n, _p(self._tk["gl"], C.c_uint8), _p(self._tk["flat"], C.c_uint8),
                                             _p(self._tk["ploidy"], C.c_int32), _p(kp, C.c_int32)))
+
+    def set_state_lists(self, lists):
+        """gp_state_lists_set: per target haplotype (targets in order, ploidy rows
+        each), the reference haplotype ids always in its target's conditioning
+        sets (the reference's --state-list rows). None or [] clears them."""
+        lists = lists or []
+        off = np.zeros(len(lists) + 1, np.int64)
+        off[1:] = np.cumsum([len(x) for x in lists])
+        ids = (np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32) for x in lists])) if lists
+               else np.zeros(1, np.int32))
+        self._check(self.lib.gp_state_lists_set(self.h, len(lists), _p(off, C.c_int64), _p(ids, C.c_int32)))
 
     def iteration(self, stage, iteration):
         self._check(self.lib.gp_iteration(self.h, stage, iteration))

@@ -103,6 +103,21 @@ const char* gp_last_error(const gp_ctx* ctx);
 int gp_targets_set(gp_ctx* ctx, int32_t n, const uint8_t* gl, const uint8_t* flat, const int32_t* ploidy,
                    const int32_t* kpbwt);
 
+/* Conditioning states always present (--state-list, caller_parameters.cpp:73;
+ * haplotype_set::read_list_states, haplotype_set.cpp:835-857). Row h lists
+ * reference haplotype ids for target haplotype h (targets in gp_targets_set
+ * order, ploidy rows each): ids[offsets[h] .. offsets[h+1]), n_haps = the sum
+ * of the ploidies. Every conditioning set of a target then also holds its
+ * rows' ids, sorted and without duplicates, except the whole-panel set of
+ * Kpbwt >= n_ref_haps (conditioning_set::compactSelection,
+ * conditioning_set.cpp:105-121). With lists, cfg->kinit and Kpbwt may be 0:
+ * that stage's set is the list alone. gp_targets_set clears the lists;
+ * n_haps = 0 clears them too. GP_E_ARG for a row count other than the
+ * targets' haplotypes, an empty row (the reference's "List of states for
+ * haplotype h is empty") or an id outside [0, n_ref_haps); at selection, for a
+ * stage whose K plus the longest list exceeds 2048 states. */
+int gp_state_lists_set(gp_ctx* ctx, int32_t n_haps, const int64_t* offsets, const int32_t* ids);
+
 /* Target GL input (genotype_reader::readTargetGenotypes, genotype_reader.cpp:427-500):
  * the FORMAT/PL (int32) or FORMAT/GL (float) values of n targets at L sites,
  * as htslib's bcf_get_format_int32 / bcf_get_format_float return them per

@@ -72,6 +72,7 @@ def ref_lib():
         lib.orc_select.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_uint32), C.c_int]
         lib.orc_init_select.argtypes = [vp, C.c_int]
         lib.orc_init_states.argtypes = [vp, C.c_int, C.POINTER(C.c_int32), C.c_int]
+        lib.orc_state_lists.argtypes = [vp, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
         lib.orc_impute.argtypes = [vp, C.POINTER(C.c_uint32), C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_uint8),
                                    C.POINTER(C.c_float), C.POINTER(C.c_int32)]
         lib.orc_rephase.argtypes = [vp, C.POINTER(C.c_uint32), C.c_int, C.POINTER(C.c_uint8), C.POINTER(C.c_uint8),
@@ -233,6 +234,16 @@ class RefOracle:
 
     def init_select(self, iter_index=0):
         self._check(self.lib.orc_init_select(self.h, iter_index))
+
+    def set_state_lists(self, lists):
+        """Per target haplotype (rows of --state-list), reference haplotype ids;
+        None or [] clears."""
+        lists = lists or []
+        off = np.zeros(len(lists) + 1, np.int64)
+        off[1:] = np.cumsum([len(x) for x in lists])
+        ids = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32) for x in lists]) if lists
+                                   else np.zeros(1, np.int32))
+        self._check(self.lib.orc_state_lists(self.h, len(lists), _p(off, C.c_int64), _p(ids, C.c_int32)))
 
     def init_states(self, ind):
         out = np.zeros(self.panel.n_ref_haps, np.int32)

@@ -463,6 +463,17 @@ int orc_init_select(void* p, int iter_index) {
     init_selection(*o, iter_index);
   });
 }
+// haplotype_set::read_list_states (haplotype_set.cpp:835-857) from memory: row
+// h of the --state-list file is ids[off[h] .. off[h+1]). n_haps = 0 clears.
+int orc_state_lists(void* p, int n_haps, const int64_t* off, const int32_t* ids) {
+  Oracle* o = static_cast<Oracle*>(p);
+  return guarded(o, [&]() {
+    haplotype_set& H = o->H;
+    H.list_states.assign(H.n_tar_haps, std::vector<int>());
+    for (int h = 0; h < n_haps && h < (int)H.n_tar_haps; ++h) H.list_states[h].assign(ids + off[h], ids + off[h + 1]);
+  });
+}
+
 int orc_init_states(void* p, int ind, int32_t* out, int cap) {
   Oracle* o = static_cast<Oracle*>(p);
   const auto& s = o->H.init_states[ind];

@@ -23,7 +23,7 @@ def test_invalid_target_arguments_are_refused(small_workload):
         bad[0] = 3
         with pytest.raises(native.GpError, match="ploidy"):
             ctx.set_targets_raw(T.n, T.gl.ctypes.data, T.flat.ctypes.data, bad.ctypes.data, 0)
-        # Kpbwt 0 needs a state list, which this path does not take
+        # Kpbwt 0 without a state list (gp_state_lists_set) is refused
         ctx.set_targets(T, kpbwt=np.zeros(T.n, np.int32))
         ctx.iteration(native.STAGE_INIT, 0)
         with pytest.raises(native.GpError, match="state list"):

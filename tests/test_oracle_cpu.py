@@ -155,3 +155,27 @@ def test_reference_driver_runs(small_workload):
         assert cnt == 2
         ds.append(g1 + 2 * np.clip(1 - g0 - g1, 0, 1))
     assert synth.dosage_r2(np.stack(ds), w.targets.truth.sum(1)) > 0.5
+
+
+def test_reference_state_lists(small_workload):
+    """The reference's --state-list path as the oracle runs it
+    (conditioning_set.cpp:114-121): every set holds the union of its target's
+    rows, sorted without duplicates; with Kinit = Kpbwt = 0 it is that union."""
+    O = _ref()
+    P, T = small_workload.panel, small_workload.targets
+    rng = np.random.default_rng(2)
+    lists = [np.sort(rng.choice(P.n_ref_haps, int(rng.integers(1, 30)), replace=False)).astype(np.int32)
+             for _ in range(int(T.ploidy.sum()))]
+    first = np.concatenate([[0], np.cumsum(T.ploidy)])
+    for kinit, kp in ((200, 150), (0, 0)):
+        orc = O.RefOracle(P, T, kinit=kinit, kpbwt=kp, kpbwt_target=np.full(T.n, kp, np.int32), pbwt_depth=8,
+                          pbwt_modulo_cm=0.05)
+        orc.set_state_lists(lists)
+        for stage, it in ((O.STAGE_INIT, 0), (O.STAGE_BURN, 1)):
+            orc.iteration(stage, it)
+            for t in range(T.n):
+                s = orc.last_states(t).astype(np.int64)
+                rows = np.unique(np.concatenate(lists[first[t]:first[t + 1]]))
+                assert np.all(np.diff(s) > 0) and np.isin(rows, s).all()
+                if kinit == 0:
+                    assert np.array_equal(s, rows)
