@@ -41,8 +41,24 @@ from glimpse_b200 import synth  # noqa: E402
 METRIC = "samples/s at matched dosage r2 (plain batched GPU path); HMM cells/s vs HBM peak"
 BURNIN, MAIN = 5, 15
 N_ITER = 1 + BURNIN + MAIN
-WORKLOAD = ("batched: 10,000 reference haplotypes x 150,000 sites over 4 Mb (80% rare, sparse), 256 diploid "
-            "targets at 0.5-2x coverage, Kpbwt 400-1200 per target, Kinit 1000, 1 init + 5 burn-in + 15 main")
+
+
+def workload_label(name):
+    """The workload's shape in words, from its entry in synth.CONFIGS."""
+    from glimpse_b200 import synth
+    c = synth.CONFIGS[name]
+
+    def spec(x, unit=""):
+        kind = x[0]
+        if kind == "fixed":
+            return f"{x[1]:g}{unit}"
+        if kind in ("uniform", "loguniform"):
+            return f"{x[1]:g}-{x[2]:g}{unit}" + (" (log-uniform)" if kind == "loguniform" else "")
+        return " / ".join(f"{v:g}{unit} ({p:.0%})" for v, p in x[1:])
+
+    return (f"{name}: {c['n_ref_haps']:,} reference haplotypes x {c['n_sites']:,} sites over {c['region_mb']:g} Mb "
+            f"({c['rare_frac']:.0%} rare, sparse), {c['n_targets']} diploid targets at {spec(c['cov'], 'x')} "
+            f"coverage, Kpbwt {spec(c['k'])} per target, Kinit {c['kinit']}, 1 init + {BURNIN} burn-in + {MAIN} main")
 
 
 def env_rank():
@@ -216,7 +232,7 @@ def run_reference(args):
     line = {"metric": METRIC, "value": value, "unit": "samples/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_run * 1000.0, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "parallelism": f"{threads} host threads",
+            "config": {"workload": workload_label(args.config), "parallelism": f"{threads} host threads",
                        "targets_timed": ref.sub.n},
             "dosage_r2": ref.dosage_r2(),
             "cpu_baseline": {"value": value, "unit": "samples/s", "cores": threads, "kind": "reference",
@@ -338,7 +354,7 @@ def run_ours(args):
     line = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "targets_per_gpu": T.n, "iterations_per_step": N_ITER,
+            "config": {"workload": workload_label(args.config), "targets_per_gpu": T.n, "iterations_per_step": N_ITER,
                        "l2": "no flush: per-step working set (alpha store, prefix arrays) is tens of GB >> 126 MB L2",
                        "parallelism": f"targets per GPU, {world} rank(s), no collective on the data path"},
             "precision": {"full": "every forward row in FP32 (as the reference)",

@@ -132,6 +132,8 @@ struct Context {
   int pbwt_states_get(int target, int32_t* counts, int32_t* states, int cap);
   int learned_prepare_panel();
   int learned_features(int Kpc, DevBuf& xout);
+  int learned_prepare_features(int Kpc);
+  int learned_feature_rows(int Kpc, DevBuf& xout, int t0, int nc);
   int learned_select_states(int stage, int iteration, int& Kp);
   int learned_labels(int Kpc, float kpos, DevBuf& yout, DevBuf& wout);
   int learned_apply_k(bool reset_state = false);

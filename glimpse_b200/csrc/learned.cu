@@ -81,7 +81,8 @@ struct FeatArgs {
   const int32_t* kfinal;
   const int32_t* urank;  // [n][N]: PBWT level << 16 | insertion index of the candidate in the union
   int N, depth;
-  __nv_bfloat16* x;  // rows ((t * nwin + w) * Kpc + k), kMlpInP columns
+  int t0;            // first target of the launch (blockIdx.z = t - t0)
+  __nv_bfloat16* x;  // rows (((t - t0) * nwin + w) * Kpc + k), kMlpInP columns
 };
 
 __device__ __forceinline__ uint32_t valid_mask(int wi, int n_com) {
@@ -120,10 +121,10 @@ __device__ int run_up(const uint32_t* cr, const uint32_t* th, int pos, int W, in
 
 // One thread per (target, window, candidate): the kMlpIn features, as BF16.
 __global__ void __launch_bounds__(128) k_features(FeatArgs a) {
-  const int t = blockIdx.z, w = blockIdx.y;
+  const int t = a.t0 + blockIdx.z, w = blockIdx.y;
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= a.Kpc) return;
-  __nv_bfloat16* row = a.x + (((size_t)t * a.nwin + w) * a.Kpc + k) * kMlpInP;
+  __nv_bfloat16* row = a.x + (((size_t)blockIdx.z * a.nwin + w) * a.Kpc + k) * kMlpInP;
   float f[kMlpInP];
 #pragma unroll
   for (int i = 0; i < kMlpInP; ++i) f[i] = 0.f;
@@ -571,6 +572,17 @@ int Context::learned_prepare_panel() {
 // The candidates of the last PBWT selection (impute.states, stride Kpc) into
 // learned.cand, and features for every (target, window, candidate) into x.
 int Context::learned_features(int Kpc, DevBuf& xout) {
+  int rc = learned_prepare_features(Kpc);
+  if (rc != GP_OK) return rc;
+  cudaError_t e;
+  if ((e = xout.ensure((size_t)tw.n * learned.nwin * Kpc * kMlpInP * 2)) != cudaSuccess)
+    return cuda_fail(e, "learned features alloc");
+  return learned_feature_rows(Kpc, xout, 0, tw.n);
+}
+
+// What the feature rows of every target read: the candidates (the PBWT
+// selection's states), the targets' bit planes and the candidates' PBWT ranks.
+int Context::learned_prepare_features(int Kpc) {
   LearnedWork& lw = learned;
   TargetWork& T = tw;
   ImputeWork& w = impute;
@@ -579,8 +591,6 @@ int Context::learned_features(int Kpc, DevBuf& xout) {
   if ((e = lw.cand.ensure((size_t)n * Kpc * 4)) != cudaSuccess) return cuda_fail(e, "learned alloc");
   if ((e = lw.ncand.ensure((size_t)n * 4)) != cudaSuccess) return cuda_fail(e, "learned alloc");
   if ((e = lw.planes.ensure((size_t)n * kPlanes * W * 4)) != cudaSuccess) return cuda_fail(e, "learned alloc");
-  const size_t rows = (size_t)n * lw.nwin * Kpc;
-  if ((e = xout.ensure(rows * kMlpInP * 2)) != cudaSuccess) return cuda_fail(e, "learned features alloc");
   if ((e = lw.urank.ensure((size_t)n * host.N * 4)) != cudaSuccess) return cuda_fail(e, "learned alloc");
   if (!pbwt_active) cudaMemsetAsync(lw.urank.ptr, 0, (size_t)n * host.N * 4, stream);  // whole panel: no union
   cudaMemcpyAsync(lw.cand.ptr, w.states.ptr, (size_t)n * Kpc * 4, cudaMemcpyDeviceToDevice, stream);
@@ -589,9 +599,16 @@ int Context::learned_features(int Kpc, DevBuf& xout) {
                                                                T.gl.as<uint8_t>(), T.flat.as<uint8_t>(),
                                                                T.ploidy.as<int32_t>(), pbwt.common2tot, host.n_com, W,
                                                                host.L, lw.planes.as<uint32_t>());
+  prof.kernel_launches += 1;
+  return cudaGetLastError() == cudaSuccess ? GP_OK : cuda_fail(cudaGetLastError(), "learned planes launch");
+}
+
+// Feature rows of targets [t0, t0 + nc) into xout from its first row.
+int Context::learned_feature_rows(int Kpc, DevBuf& xout, int t0, int nc) {
+  LearnedWork& lw = learned;
   FeatArgs fa;
   fa.refT = panel.refT;
-  fa.W = W;
+  fa.W = panel.W;
   fa.n_com = host.n_com;
   fa.nwin = lw.nwin;
   fa.Kpc = Kpc;
@@ -602,9 +619,10 @@ int Context::learned_features(int Kpc, DevBuf& xout) {
   fa.urank = lw.urank.as<int32_t>();
   fa.N = host.N;
   fa.depth = cfg.pbwt_depth;
+  fa.t0 = t0;
   fa.x = xout.as<__nv_bfloat16>();
-  k_features<<<dim3((Kpc + 127) / 128, lw.nwin, n), 128, 0, stream>>>(fa);
-  prof.kernel_launches += 2;
+  k_features<<<dim3((Kpc + 127) / 128, lw.nwin, nc), 128, 0, stream>>>(fa);
+  prof.kernel_launches += 1;
   return cudaGetLastError() == cudaSuccess ? GP_OK : cuda_fail(cudaGetLastError(), "learned features launch");
 }
 
@@ -623,15 +641,28 @@ int Context::learned_select_states(int stage, int iteration, int& Kp) {
   if ((e0 = w.nstates.ensure((size_t)n * 4)) != cudaSuccess) return cuda_fail(e0, "alloc nstates");
   int rc = pbwt_select_states(stage, iteration, Kpc);
   if (rc != GP_OK) return rc;
-  rc = learned_features(Kpc, lw.x);
+  rc = learned_prepare_features(Kpc);
   if (rc != GP_OK) return rc;
-  const size_t rows = (size_t)n * lw.nwin * Kpc;
+  const size_t per_t = (size_t)lw.nwin * Kpc;  // feature rows of one target
+  const size_t rows = (size_t)n * per_t;
   cudaError_t e;
   if ((e = lw.score.ensure(rows * 4)) != cudaSuccess) return cuda_fail(e, "learned alloc");
   if ((e = lw.best.ensure((size_t)n * Kpc * 4)) != cudaSuccess) return cuda_fail(e, "learned alloc");
   if ((e = lw.cnt.ensure((size_t)n * Kpc * 4)) != cudaSuccess) return cuda_fail(e, "learned alloc");
-  rc = mlp_forward_device(*this, lw.x.as<__nv_bfloat16>(), (int)rows, lw.score.as<float>(), nullptr, nullptr);
-  if (rc != GP_OK) return rc;
+  // Feature rows and their scores in chunks of targets whose rows fit the
+  // memory budget (the rows are 128 B each; the scores are kept for all).
+  const size_t row_bytes = (size_t)kMlpInP * 2;
+  const size_t budget = store_budget(lw.x.cap, rows * row_bytes);
+  const int nc = (int)std::max<size_t>(1, std::min<size_t>(n, budget / (per_t * row_bytes)));
+  if ((e = lw.x.ensure((size_t)nc * per_t * row_bytes)) != cudaSuccess) return cuda_fail(e, "learned features alloc");
+  for (int t0 = 0; t0 < n; t0 += nc) {
+    const int m = std::min(nc, n - t0);
+    rc = learned_feature_rows(Kpc, lw.x, t0, m);
+    if (rc != GP_OK) return rc;
+    rc = mlp_forward_device(*this, lw.x.as<__nv_bfloat16>(), (int)((size_t)m * per_t),
+                            lw.score.as<float>() + (size_t)t0 * per_t, nullptr, nullptr);
+    if (rc != GP_OK) return rc;
+  }
   if ((e = lw.maxs.ensure((size_t)n * Kpc * 4)) != cudaSuccess) return cuda_fail(e, "learned alloc");
   cudaMemsetAsync(lw.maxs.ptr, 0x80, (size_t)n * Kpc * 4, stream);  // below every score's key
   cudaMemsetAsync(lw.best.ptr, 0x7F, (size_t)n * Kpc * 4, stream);
