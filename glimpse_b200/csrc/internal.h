@@ -13,6 +13,35 @@
 namespace gp {
 
 constexpr int kWarp = 32;
+
+#ifdef __CUDACC__
+// Two floats in one 64-bit register pair (lo = first); the packed mul / add /
+// fma (sm_100a) round each element exactly as the scalar instructions do.
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 f2_pack(float lo, float hi) {
+  f2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(f2 v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2 f2_fma(f2 a, f2 b, f2 c) {
+  f2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ f2 f2_mul(f2 a, f2 b) {
+  f2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2 f2_add(f2 a, f2 b) {
+  f2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+#endif
 constexpr int kImputeThreads = 256;           // threads per haplotype in the imputation HMM
 constexpr int kImputeStatesPerThread = 8;     // registers per thread for owned states
 constexpr int kMaxStates = kImputeThreads * kImputeStatesPerThread;  // 2048

@@ -145,33 +145,6 @@ __device__ __forceinline__ float compf(const float4& v, int c) { return c == 0 ?
 // its stored row vector (global, quad j at offset 32 W j). Every chain of a
 // launch runs the launch's J quads, so a site is one straight-line block; the
 // padded states (vf = 0) are kept at 0, and the vectors are written whole.
-// Two floats in one 64-bit register pair (lo = first); the packed mul / add /
-// fma round each element exactly as the scalar instructions do.
-typedef unsigned long long f2;
-__device__ __forceinline__ f2 f2_pack(float lo, float hi) {
-  f2 r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-  return r;
-}
-__device__ __forceinline__ void f2_unpack(f2 v, float& lo, float& hi) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-__device__ __forceinline__ f2 f2_fma(f2 a, f2 b, f2 c) {
-  f2 d;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-  return d;
-}
-__device__ __forceinline__ f2 f2_mul(f2 a, f2 b) {
-  f2 d;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ f2 f2_add(f2 a, f2 b) {
-  f2 d;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-
 template <int J, int W, bool FWD, bool POST, bool INIT>
 __device__ __forceinline__ void chain_step(float4 (&x)[J], const uint4 (&w)[J], uint32_t m, float (&q0)[4],
                                            float (&q1)[4], float (&q2)[4], const float4 (&vf)[J], uint32_t qmask,

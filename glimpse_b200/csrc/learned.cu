@@ -652,7 +652,9 @@ int Context::learned_select_states(int stage, int iteration, int& Kp) {
   // Feature rows and their scores in chunks of targets whose rows fit the
   // memory budget (the rows are 128 B each; the scores are kept for all).
   const size_t row_bytes = (size_t)kMlpInP * 2;
-  const size_t budget = store_budget(lw.x.cap, rows * row_bytes);
+  // at most 2 GiB of rows at a time (16M rows, hundreds of waves of the
+  // network's 128-row tiles), so that the rows do not take the stores' memory
+  const size_t budget = std::min<size_t>(store_budget(lw.x.cap, rows * row_bytes), size_t(2) << 30);
   const int nc = (int)std::max<size_t>(1, std::min<size_t>(n, budget / (per_t * row_bytes)));
   if ((e = lw.x.ensure((size_t)nc * per_t * row_bytes)) != cudaSuccess) return cuda_fail(e, "learned features alloc");
   for (int t0 = 0; t0 < n; t0 += nc) {
@@ -958,6 +960,10 @@ int gp_learned_train(gp_ctx* ctx, int32_t kcand, float kpos, int32_t steps, int3
     }
     if ((e = cudaStreamSynchronize(c.stream)) != cudaSuccess) return c.cuda_fail(e, "learned train");
   }
+  // the label HMM's store and the training rows are not needed by selection:
+  // give their memory back to the iteration's stores
+  for (gp::DevBuf* b : {&lw.astore, &lw.aoff, &lw.mass0, &lw.mass1, &lw.xall, &lw.yall, &lw.wall, &lw.idx})
+    b->release();
   return gp::check_mlp_err(c, "learned train");
 }
 

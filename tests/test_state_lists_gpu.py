@@ -53,12 +53,13 @@ def test_state_lists_iterations_match_reference(small_workload, kinit, kpbwt):
             gh0, gh1 = ctx.haps()
             for t in range(T.n):
                 s = ctx.states(t)
-                assert np.array_equal(orc.last_states(t), s), (stage, t)
                 rows = np.unique(np.concatenate(lists[first[t]:first[t + 1]]))
-                whole = kpbwt == "panel" and stage == O.STAGE_BURN
-                if whole:
+                if kpbwt == "panel" and stage == O.STAGE_BURN:
+                    # the reference builds the whole-panel set once per worker and
+                    # leaves idxHaps_ref empty on later calls (conditioning_set.cpp:105-113)
                     assert np.array_equal(s, np.arange(P.n_ref_haps))
                 else:
+                    assert np.array_equal(orc.last_states(t), s), (stage, t)
                     assert np.isin(rows, s).all()
                 if kinit == 0:
                     assert np.array_equal(s, rows)
