@@ -360,7 +360,8 @@ def run_ours(args):
             "precision": {"full": "every forward row in FP32 (as the reference)",
                           "f32": "FP32 checkpoints every 32 sites, recompute",
                           "bf16": "BF16 checkpoints every 32 sites, FP32 recompute"}[args.precision],
-            "autotuned": dict(zip(("chains_per_cta", "sweep_haps_per_warp"), ctx.tuning()[:2])),
+            "autotuned": dict(zip(("chains_per_cta", "sweep_haps_per_warp", "phase_placement", "ms"),
+                                  (lambda tu: (*tu[:3], [round(float(x), 3) for x in tu[3]]))(ctx.tuning()))),
             "hmm_cells_per_s": world * hmm_cells / (ms / 1000.0),
             "dosage_r2": r2,
             "gpu_launches": int(prof["kernel_launches"]),

@@ -533,6 +533,26 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
     Kmax = std::max(Kmax, host_nstates[t]);
   }
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+  // Placement 2, for batches of one to two entries per SM: the CTAs at grid
+  // positions i and S + i share an SM (S SMs, two CTAs per SM), so the heaviest
+  // 2S - nb entries take positions nb - S .. S - 1 and run alone, and the rest
+  // are paired heaviest with lightest.
+  if (sm_count == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
+  }
+  const int S_sm = sm_count;
+  std::vector<int32_t> order_paired;
+  if (nb > S_sm && nb <= 2 * S_sm) {
+    const int npair = nb - S_sm, nsolo = S_sm - npair;
+    order_paired.assign(nb, 0);
+    for (int j = 0; j < nsolo; ++j) order_paired[npair + j] = order[j];
+    for (int j = 0; j < npair; ++j) {
+      order_paired[j] = order[nsolo + j];
+      order_paired[S_sm + j] = order[nb - 1 - j];
+    }
+  }
   // The per-entry buffers of fixed size come first, so that the budget below
   // sees the memory they leave.
   if ((e = p.offs.ensure((size_t)nb * 2 * 8)) != cudaSuccess) return cuda_fail(e, "alloc offs");
@@ -575,7 +595,10 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   std::vector<int64_t> offs(poff);
   offs.insert(offs.end(), ioff.begin(), ioff.end());
   cudaMemcpyAsync(p.offs.ptr, offs.data(), offs.size() * 8, cudaMemcpyHostToDevice, stream);
-  cudaMemcpyAsync(p.order.ptr, order.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, stream);
+  const int porder = fixed_porder ? fixed_porder : tune_porder;
+  const bool paired_ok = !order_paired.empty() && chunk_start.size() == 2;
+  cudaMemcpyAsync(p.order.ptr, (paired_ok && porder == 2 ? order_paired : order).data(), (size_t)nb * 4,
+                  cudaMemcpyHostToDevice, stream);
   PhaseStore S;
   S.pprob = p.pool.as<float>();
   S.pprob_off = p.offs.as<int64_t>();
@@ -595,6 +618,43 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
     pcells += 2.0 * 8.0 * (double)cnt[b] * (double)host_nstates[t];
   }
   launch_var_records(d_tsel, nb, w.poly.as<int32_t>(), L, panel.cm, mc, V, stream);
+  if (paired_ok && porder == 0) {
+    // Autotune the placement: k_phase reads only its inputs and rewrites its
+    // own outputs, so it runs once per candidate and the results are the same.
+    if ((e = p.order2.ensure((size_t)nb * 4)) != cudaSuccess) return cuda_fail(e, "alloc order");
+    cudaMemcpyAsync(p.order2.ptr, order_paired.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, stream);
+    cudaEvent_t e0, e1, e2;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventCreate(&e2);
+    PhaseStore S2 = S;
+    S2.order = p.order2.as<int32_t>();
+    cudaEventRecord(e0, stream);
+    int lrc = launch_phase(J, d_tsel, nb, w.nstates.as<int32_t>(), w.hvar.as<uint32_t>(), w.WB, w.Kp,
+                           w.poly.as<int32_t>(), w.npoly.as<int32_t>(), L, panel.cm, V, S, mc, cfg.seed, iteration,
+                           d_target_ids, stream);
+    cudaEventRecord(e1, stream);
+    if (lrc == GP_OK)
+      lrc = launch_phase(J, d_tsel, nb, w.nstates.as<int32_t>(), w.hvar.as<uint32_t>(), w.WB, w.Kp,
+                         w.poly.as<int32_t>(), w.npoly.as<int32_t>(), L, panel.cm, V, S2, mc, cfg.seed, iteration,
+                         d_target_ids, stream);
+    cudaEventRecord(e2, stream);
+    const cudaError_t es = cudaEventSynchronize(e2);
+    float m1 = 0.f, m2 = 0.f;
+    cudaEventElapsedTime(&m1, e0, e1);
+    cudaEventElapsedTime(&m2, e1, e2);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    if (lrc != GP_OK) return (fail(GP_E_ARG, "phasing: too many states"), GP_E_ARG);
+    if (es != cudaSuccess) return cuda_fail(es, "phasing placement tuning");
+    prof.kernel_launches += 2;
+    tune_ms[7] = m1;
+    tune_ms[8] = m2;
+    tune_porder = m2 < m1 ? 2 : 1;
+    if (tune_porder == 2)
+      cudaMemcpyAsync(p.order.ptr, p.order2.ptr, (size_t)nb * 4, cudaMemcpyDeviceToDevice, stream);
+  }
   cudaEvent_t ea;
   prof_begin(ea);
   for (size_t c = 0; c + 1 < chunk_start.size(); ++c) {
@@ -685,28 +745,34 @@ const char* gp_last_error(const gp_ctx* ctx) {
   return ctx ? reinterpret_cast<const Context*>(ctx)->err.c_str() : "null context";
 }
 
-int gp_tuning_set(gp_ctx* ctx, int32_t chains_per_cta, int32_t sweep_haps_per_warp) {
+int gp_tuning_set(gp_ctx* ctx, int32_t chains_per_cta, int32_t sweep_haps_per_warp, int32_t phase_placement) {
   if (!ctx) return GP_E_ARG;
   Context& c = *reinterpret_cast<Context*>(ctx);
   if ((chains_per_cta != 0 && chains_per_cta != 1 && chains_per_cta != 2 && chains_per_cta != 4) ||
       (sweep_haps_per_warp != 0 && sweep_haps_per_warp != 1 && sweep_haps_per_warp != 2 && sweep_haps_per_warp != 4 &&
-       sweep_haps_per_warp != 8))
-    return (c.fail(GP_E_ARG, "tuning: chains per CTA in {0, 1, 2, 4}, haplotypes per sweep warp in {0, 1, 2, 4, 8}"),
+       sweep_haps_per_warp != 8) ||
+      phase_placement < 0 || phase_placement > 2)
+    return (c.fail(GP_E_ARG, "tuning: chains per CTA in {0, 1, 2, 4}, haplotypes per sweep warp in {0, 1, 2, 4, 8}, "
+                             "phasing placement in {0, 1, 2}"),
             GP_E_ARG);
   c.fixed_cpc = chains_per_cta;
   c.fixed_hpw = sweep_haps_per_warp;
+  c.fixed_porder = phase_placement;
   if (!chains_per_cta) c.tune_cpc = 0;
   if (!sweep_haps_per_warp) c.tune_hpw = 0;
+  if (!phase_placement) c.tune_porder = 0;
   return GP_OK;
 }
 
-int gp_tuning_get(gp_ctx* ctx, int32_t* chains_per_cta, int32_t* sweep_haps_per_warp, float* ms) {
+int gp_tuning_get(gp_ctx* ctx, int32_t* chains_per_cta, int32_t* sweep_haps_per_warp, int32_t* phase_placement,
+                  float* ms) {
   if (!ctx) return GP_E_ARG;
   Context& c = *reinterpret_cast<Context*>(ctx);
   if (chains_per_cta) *chains_per_cta = c.fixed_cpc ? c.fixed_cpc : c.tune_cpc;
   if (sweep_haps_per_warp) *sweep_haps_per_warp = c.fixed_hpw ? c.fixed_hpw : c.tune_hpw;
+  if (phase_placement) *phase_placement = c.fixed_porder ? c.fixed_porder : c.tune_porder;
   if (ms)
-    for (int i = 0; i < 7; ++i) ms[i] = c.tune_ms[i];
+    for (int i = 0; i < 9; ++i) ms[i] = c.tune_ms[i];
   return GP_OK;
 }
 

@@ -377,15 +377,15 @@ class Context:
                                                _p(wt, C.c_float), C.c_float(lr), C.byref(loss), _p(g, C.c_float)))
         return loss.value, g
 
-    def tuning_set(self, chains_per_cta=0, sweep_haps_per_warp=0):
-        self._check(self.lib.gp_tuning_set(self.h, chains_per_cta, sweep_haps_per_warp))
+    def tuning_set(self, chains_per_cta=0, sweep_haps_per_warp=0, phase_placement=0):
+        self._check(self.lib.gp_tuning_set(self.h, chains_per_cta, sweep_haps_per_warp, phase_placement))
 
     def tuning(self):
-        """(chains per CTA, haplotypes per sweep warp, measured ms[7]) of the autotuner."""
-        a, b = C.c_int32(0), C.c_int32(0)
-        ms = np.zeros(7, np.float32)
-        self._check(self.lib.gp_tuning_get(self.h, C.byref(a), C.byref(b), _p(ms, C.c_float)))
-        return a.value, b.value, ms
+        """(chains per CTA, haplotypes per sweep warp, phasing placement, measured ms[9]) of the autotuner."""
+        a, b, c = C.c_int32(0), C.c_int32(0), C.c_int32(0)
+        ms = np.zeros(9, np.float32)
+        self._check(self.lib.gp_tuning_get(self.h, C.byref(a), C.byref(b), C.byref(c), _p(ms, C.c_float)))
+        return a.value, b.value, c.value, ms
 
     def set_precision(self, mode):
         """gp_set_precision: PRECISION_FULL, PRECISION_CKPT_F32 or PRECISION_CKPT_BF16."""

@@ -124,9 +124,40 @@ def test_autotuned_shapes_do_not_change_results():
             assert np.array_equal(ctxs[0].states(t), ctxs[2].states(t))
         h = [c.haps() for c in ctxs]
         assert np.array_equal(h[0][0], h[1][0]) and np.array_equal(h[0][1], h[2][1])
-        cpc, hpw, ms = ctxs[2].tuning()
+        cpc, hpw, _, ms = ctxs[2].tuning()
         assert cpc in (1, 2, 4) and hpw in (1, 2, 4, 8)
-        assert (ms[:3] != 0).any() and (ms[3:] > 0).all()
+        assert (ms[:3] != 0).any() and (ms[3:7] > 0).all()
+    finally:
+        for c in ctxs:
+            c.close()
+
+
+@pytest.mark.gpu
+def test_phasing_placement_does_not_change_results():
+    """A batch of one to two targets per SM: the phasing placements (decreasing
+    work; heaviest alone, the rest paired) give identical haplotypes, and the
+    autotuner times both and reports its choice."""
+    import torch
+    from glimpse_b200 import native, synth
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    n = sms + sms // 2
+    w = synth.make_panel_and_targets(600, 3000, 0.3, 0.5, n, ("uniform", 0.5, 2.0), ("uniform", 60, 300), seed=43,
+                                     sparse_maf=0.01)
+    P, T = w.panel, w.targets
+    kw = dict(kinit=150, kpbwt=int(T.kpbwt.max()), pbwt_depth=8, pbwt_modulo_cm=0.05)
+    ctxs = [native.Context(P, **kw) for _ in range(3)]
+    try:
+        ctxs[0].tuning_set(0, 0, 1)
+        ctxs[1].tuning_set(0, 0, 2)
+        for c in ctxs:
+            c.set_targets(T, kpbwt=T.kpbwt)
+            c.iteration(native.STAGE_INIT, 0)
+            c.iteration(native.STAGE_BURN, 1)
+        h = [c.haps() for c in ctxs]
+        for i in (1, 2):
+            assert np.array_equal(h[0][0], h[i][0]) and np.array_equal(h[0][1], h[i][1])
+        _, _, placement, ms = ctxs[2].tuning()
+        assert placement in (1, 2) and ms[7] > 0 and ms[8] > 0
     finally:
         for c in ctxs:
             c.close()
