@@ -525,12 +525,13 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   // heaviest targets start first and share an SM with the lightest.
   std::vector<int32_t> order(nb);
   std::vector<double> cost(nb);
-  int Kmax = 0;
+  int Kmax = 0, Kmin = 1 << 30;
   for (int b = 0; b < nb; ++b) {
     const int t = tsel_host.empty() ? b : tsel_host[b];
     order[b] = b;
     cost[b] = (double)cnt[b] * (1.0 + (double)((host_nstates[t] + kPhaseThreads - 1) / kPhaseThreads));
     Kmax = std::max(Kmax, host_nstates[t]);
+    Kmin = std::min(Kmin, host_nstates[t]);
   }
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
   // Placement 2, for batches of one to two entries per SM: the CTAs at grid
@@ -618,9 +619,10 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
     pcells += 2.0 * 8.0 * (double)cnt[b] * (double)host_nstates[t];
   }
   launch_var_records(d_tsel, nb, w.poly.as<int32_t>(), L, panel.cm, mc, V, stream);
-  if (paired_ok && porder == 0) {
-    // Autotune the placement: k_phase reads only its inputs and rewrites its
-    // own outputs, so it runs once per candidate and the results are the same.
+  if (paired_ok && porder == 0 && Kmin != Kmax) {
+    // Autotune the placement on the first batch whose entries' state counts
+    // differ (where their work differs most): k_phase reads only its inputs and
+    // rewrites its own outputs, so it runs once per candidate with the same results.
     if ((e = p.order2.ensure((size_t)nb * 4)) != cudaSuccess) return cuda_fail(e, "alloc order");
     cudaMemcpyAsync(p.order2.ptr, order_paired.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, stream);
     cudaEvent_t e0, e1, e2;

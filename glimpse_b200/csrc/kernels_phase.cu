@@ -203,52 +203,6 @@ __device__ __forceinline__ void block_sum8(float (&v)[8], float (*red)[NW][8], i
   buf ^= 1;
 }
 
-// Warp reduce-scatter of 32 values: halving exchanges over lane bits 4..0 leave
-// lane L with the warp sum of value L (31 shuffles in place of 32 reductions).
-__device__ __forceinline__ float warp_scatter32(const float (&v)[32]) {
-  const int lane = threadIdx.x & 31;
-  float a[16], b[8], c[4], d[2];
-  bool up = lane & 16;
-#pragma unroll
-  for (int i = 0; i < 16; ++i)
-    a[i] = __fadd_rn(up ? v[i + 16] : v[i], __shfl_xor_sync(0xffffffffu, up ? v[i] : v[i + 16], 16));
-  up = lane & 8;
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-    b[i] = __fadd_rn(up ? a[i + 8] : a[i], __shfl_xor_sync(0xffffffffu, up ? a[i] : a[i + 8], 8));
-  up = lane & 4;
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-    c[i] = __fadd_rn(up ? b[i + 4] : b[i], __shfl_xor_sync(0xffffffffu, up ? b[i] : b[i + 4], 4));
-  up = lane & 2;
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-    d[i] = __fadd_rn(up ? c[i + 2] : c[i], __shfl_xor_sync(0xffffffffu, up ? c[i] : c[i + 2], 2));
-  up = lane & 1;
-  return __fadd_rn(up ? d[1] : d[0], __shfl_xor_sync(0xffffffffu, up ? d[0] : d[1], 1));
-}
-
-// The same for 16 values: lanes L and L ^ 1 both end with the warp sum of value L >> 1.
-__device__ __forceinline__ float warp_scatter16(const float (&v)[16]) {
-  const int lane = threadIdx.x & 31;
-  float a[8], b[4], c[2];
-  bool up = lane & 16;
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-    a[i] = __fadd_rn(up ? v[i + 8] : v[i], __shfl_xor_sync(0xffffffffu, up ? v[i] : v[i + 8], 16));
-  up = lane & 8;
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-    b[i] = __fadd_rn(up ? a[i + 4] : a[i], __shfl_xor_sync(0xffffffffu, up ? a[i] : a[i + 4], 8));
-  up = lane & 4;
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-    c[i] = __fadd_rn(up ? b[i + 2] : b[i], __shfl_xor_sync(0xffffffffu, up ? b[i] : b[i + 2], 4));
-  up = lane & 2;
-  float e = __fadd_rn(up ? c[1] : c[0], __shfl_xor_sync(0xffffffffu, up ? c[0] : c[1], 2));
-  return __fadd_rn(e, __shfl_xor_sync(0xffffffffu, e, 1));
-}
-
 // horizontal_add of 8 lanes as the reference's AVX reduction orders it
 // (phasing_hmm.h:47-57): ((v0+v4)+(v1+v5)) + ((v2+v6)+(v3+v7)).
 __device__ __forceinline__ float hadd8(const float (&v)[8]) {
@@ -271,8 +225,6 @@ struct PhaseShared {
   // per VAR code: emissions of the 8 hypotheses for a state allele of 0 ([0..7]) and 1 ([8..15]); read as float4
   __align__(16) float etab[16][16];
   float red[2][NW][8];
-  float red64[NW][64];     // TRANS_HAP: per-warp sums of the 64 (h1, h2) products
-  float red16[2][NW][16];  // IMPUTE_FLAT_HET: per-warp sums of the 16 allele-split products
   float sumH[8];
   float sumT;
   float hprobs[64];
@@ -316,37 +268,25 @@ __device__ __forceinline__ void site_update(float (&prob)[J][8], const float (&s
     for (int h = 0; h < 8; ++h) tF[h] = __fmul_rn(sumH[h], sc);
     ntp = nt / sumT;
   }
-  // hypotheses (2p, 2p + 1) as packed pairs: the same roundings as the scalar
-  // fma / mul / add
-  f2 part2[4], tF2[4], e02[4], e12[4];
-  const f2 ntp2 = f2_pack(ntp, ntp);
+  float part[8];
 #pragma unroll
-  for (int p = 0; p < 4; ++p) {
-    part2[p] = f2_pack(0.f, 0.f);
-    tF2[p] = MODE != 0 ? f2_pack(tF[2 * p], tF[2 * p + 1]) : part2[p];
-    e02[p] = f2_pack(e0[2 * p], e0[2 * p + 1]);
-    e12[p] = f2_pack(e1[2 * p], e1[2 * p + 1]);
-  }
+  for (int h = 0; h < 8; ++h) part[h] = 0.f;
 #pragma unroll
   for (int j = 0; j < J; ++j) {
     const int k = tid + j * PT;
     if (k >= K) continue;
     const bool bit = (w[j] & m) != 0u;
-    const f2 sk2 = f2_pack(sumk[j], sumk[j]);
 #pragma unroll
-    for (int p = 0; p < 4; ++p) {
-      const f2 e = bit ? e12[p] : e02[p];
-      f2 v;
+    for (int h = 0; h < 8; ++h) {
+      const float e = bit ? e1[h] : e0[h];
+      float v;
       if (MODE == 0) v = e;
-      else if (MODE == 1) v = f2_mul(f2_fma(f2_pack(prob[j][2 * p], prob[j][2 * p + 1]), ntp2, tF2[p]), e);
-      else v = f2_mul(f2_fma(sk2, ntp2, tF2[p]), e);
-      f2_unpack(v, prob[j][2 * p], prob[j][2 * p + 1]);
-      part2[p] = f2_add(part2[p], v);
+      else if (MODE == 1) v = __fmul_rn(fmaf(prob[j][h], ntp, tF[h]), e);
+      else v = __fmul_rn(fmaf(sumk[j], ntp, tF[h]), e);
+      prob[j][h] = v;
+      part[h] = __fadd_rn(part[h], v);
     }
   }
-  float part[8];
-#pragma unroll
-  for (int p = 0; p < 4; ++p) f2_unpack(part2[p], part[2 * p], part[2 * p + 1]);
   block_sum8(part, red, buf, sumH);
   sumT = hadd8(sumH);
 }
@@ -446,7 +386,7 @@ __global__ void __launch_bounds__(PT, 2) k_phase(const int32_t* __restrict__ tse
                                               uint64_t seed, int iteration, const int32_t* __restrict__ target_ids) {
   __shared__ PhaseShared sm;
   __shared__ VarStage vs;
-  int buf = 0, fbuf = 0;
+  int buf = 0;
   const int b = S.order ? S.order[blockIdx.x] : blockIdx.x;
   const int t = tsel ? tsel[b] : b;
   const int K = nstates[t];
@@ -583,62 +523,37 @@ __global__ void __launch_bounds__(PT, 2) k_phase(const int32_t* __restrict__ tse
       const bool seg_end = (fl & 2) != 0;
       if (seg_end) do_sumk();
       if (seg_end && i != nv - 1) {
-        // TRANS_HAP (phasing_hmm.h:376-397): the 64 sums over states of
-        // (prob[k][h1] nt2 / sumT + sumH[h1] yt2 / (sumT K)) x next[k][h2], in two
-        // groups of four h1 (each next row read once per group), reduced in one pass
+        // TRANS_HAP (phasing_hmm.h:376-397)
         const float yt2 = V.yt_next[vbase + i];
         const float nt2 = 1.0f - yt2;
         const float fact2 = nt2 / sumT;
         const float* nxt = PP + (size_t)(seg + 1) * K * 8;
-        float fact1[8];
+        float sumHP = 0.f;
 #pragma unroll
-        for (int h1 = 0; h1 < 8; ++h1) fact1[h1] = __fmul_rn(sumH[h1] / sumT, yt2) / (float)K;
-        const int lane = tid & 31, warp = tid >> 5;
+        for (int h1 = 0; h1 < 8; ++h1) {
+          const float fact1 = __fmul_rn(sumH[h1] / sumT, yt2) / (float)K;
+          float acc[8];
 #pragma unroll
-        for (int g = 0; g < 2; ++g) {
-          float acc[32];
-#pragma unroll
-          for (int q = 0; q < 32; ++q) acc[q] = 0.f;
+          for (int h2 = 0; h2 < 8; ++h2) acc[h2] = 0.f;
 #pragma unroll
           for (int j = 0; j < J; ++j) {
             const int k = tid + j * PT;
             if (k < K) {
+              const float p0 = fmaf(prob[j][h1], fact2, fact1);
               const float4* s4 = reinterpret_cast<const float4*>(nxt + (size_t)k * 8);
               const float4 x = s4[0], y = s4[1];
-#pragma unroll
-              for (int hl = 0; hl < 4; ++hl) {
-                const float p0 = fmaf(prob[j][4 * g + hl], fact2, fact1[4 * g + hl]);
-                float* a8 = acc + 8 * hl;
-                a8[0] = fmaf(p0, x.x, a8[0]); a8[1] = fmaf(p0, x.y, a8[1]);
-                a8[2] = fmaf(p0, x.z, a8[2]); a8[3] = fmaf(p0, x.w, a8[3]);
-                a8[4] = fmaf(p0, y.x, a8[4]); a8[5] = fmaf(p0, y.y, a8[5]);
-                a8[6] = fmaf(p0, y.z, a8[6]); a8[7] = fmaf(p0, y.w, a8[7]);
-              }
+              acc[0] = fmaf(p0, x.x, acc[0]); acc[1] = fmaf(p0, x.y, acc[1]);
+              acc[2] = fmaf(p0, x.z, acc[2]); acc[3] = fmaf(p0, x.w, acc[3]);
+              acc[4] = fmaf(p0, y.x, acc[4]); acc[5] = fmaf(p0, y.y, acc[5]);
+              acc[6] = fmaf(p0, y.z, acc[6]); acc[7] = fmaf(p0, y.w, acc[7]);
             }
           }
-          sm.red64[warp][32 * g + lane] = warp_scatter32(acc);
-        }
-        __syncthreads();
-        if (warp == 0) {
-          float x0 = sm.red64[0][lane], x1 = sm.red64[0][lane + 32];
+          float tot[8];
+          block_sum8(acc, sm.red, buf, tot);
+          if (tid == 0)
 #pragma unroll
-          for (int q = 1; q < NW; ++q) {
-            x0 = __fadd_rn(x0, sm.red64[q][lane]);
-            x1 = __fadd_rn(x1, sm.red64[q][lane + 32]);
-          }
-          sm.hprobs[lane] = x0;
-          sm.hprobs[lane + 32] = x1;
-        }
-        __syncwarp();
-        float sumHP = 0.f;
-        if (tid == 0) {
-#pragma unroll
-          for (int h1 = 0; h1 < 8; ++h1) {
-            float v8[8];
-#pragma unroll
-            for (int h2 = 0; h2 < 8; ++h2) v8[h2] = sm.hprobs[h1 * 8 + h2];
-            sumHP = __fadd_rn(sumHP, hadd8(v8));
-          }
+            for (int h2 = 0; h2 < 8; ++h2) sm.hprobs[h1 * 8 + h2] = tot[h2];
+          sumHP = __fadd_rn(sumHP, hadd8(tot));
         }
         // SAMPLE_DIP (phasing_hmm.h:400-411)
         if (tid == 0) {
@@ -679,9 +594,9 @@ __global__ void __launch_bounds__(PT, 2) k_phase(const int32_t* __restrict__ tse
           sR[h] = 1.0f / IPS[m * 8 + h];
           sL[h] = 1.0f / sumH[h];
         }
-        float s01[16];  // [0, 8): state allele 0; [8, 16): state allele 1
+        float s0[8], s1[8];
 #pragma unroll
-        for (int h = 0; h < 16; ++h) s01[h] = 0.f;
+        for (int h = 0; h < 8; ++h) s0[h] = s1[h] = 0.f;
 #pragma unroll
         for (int j = 0; j < J; ++j) {
           const int k = tid + j * PT;
@@ -694,25 +609,17 @@ __global__ void __launch_bounds__(PT, 2) k_phase(const int32_t* __restrict__ tse
             for (int h = 0; h < 8; ++h) {
               const float p1 = __fmul_rn(ip[h], sR[h]);
               const float p2 = __fmul_rn(prob[j][h], sL[h]);
-              if (bit) s01[8 + h] = fmaf(p1, p2, s01[8 + h]); else s01[h] = fmaf(p1, p2, s01[h]);
+              if (bit) s1[h] = fmaf(p1, p2, s1[h]); else s0[h] = fmaf(p1, p2, s0[h]);
             }
           }
         }
-        const float r16 = warp_scatter16(s01);
-        const int lane = tid & 31;
-        if ((lane & 1) == 0) sm.red16[fbuf][tid >> 5][lane >> 1] = r16;
-        __syncthreads();
+        float t0[8], t1[8];
+        block_sum8(s0, sm.red, buf, t0);
+        block_sum8(s1, sm.red, buf, t1);
         if (tid < 8) {
-          float a0 = sm.red16[fbuf][0][tid], a1 = sm.red16[fbuf][0][tid + 8];
-#pragma unroll
-          for (int q = 1; q < NW; ++q) {
-            a0 = __fadd_rn(a0, sm.red16[fbuf][q][tid]);
-            a1 = __fadd_rn(a1, sm.red16[fbuf][q][tid + 8]);
-          }
-          const float r = a1 / __fadd_rn(a0, a1);
+          const float r = t1[tid] / __fadd_rn(t0[tid], t1[tid]);
           OF1[m * 8 + tid] = fmaxf(0.0f, fminf(1.0f, r));
         }
-        fbuf ^= 1;
       }
     }
     if (loader && have_next && ((vb + 1) << 5) + tid < nv) vs.rec[cur ^ 1][tid] = pre;
