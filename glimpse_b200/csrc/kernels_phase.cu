@@ -151,8 +151,7 @@ __global__ void k_var_records(const int32_t* __restrict__ tsel, const int32_t* _
 // ---------------------------------------------------------------------------
 // Block reduction of 8 values (one per hypothesis).
 // Within a warp a reduce-scatter leaves lane L with the warp sum of value
-// ((L>>4)&1)*4 + ((L>>3)&1)*2 + ((L>>2)&1); after the barrier every thread
-// adds the warps' partials in warp order.
+// ((L>>4)&1)*4 + ((L>>3)&1)*2 + ((L>>2)&1); warps are then combined in order.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void block_sum8(float (&v)[8], float (*red)[NW][8], int& buf, float (&out)[8]) {
   const int lane = threadIdx.x & 31;
@@ -186,18 +185,21 @@ __device__ __forceinline__ void block_sum8(float (&v)[8], float (*red)[NW][8], i
   const int warp = threadIdx.x >> 5;
   if ((lane & 3) == 0) red[buf][warp][((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1)] = c;
   __syncthreads();
-  // every thread adds the warps' partials in warp order (broadcast 16-byte loads)
-  static_assert(NW == 8, "8 warps of partials");
-  const float4* r4 = reinterpret_cast<const float4*>(red[buf][0]);
-  float4 s0 = r4[0], s1 = r4[1];
-#pragma unroll 1
-  for (int q = 1; q < NW; ++q) {
-    const float4 b0 = r4[2 * q], b1 = r4[2 * q + 1];
-    s0.x = __fadd_rn(s0.x, b0.x); s0.y = __fadd_rn(s0.y, b0.y); s0.z = __fadd_rn(s0.z, b0.z); s0.w = __fadd_rn(s0.w, b0.w);
-    s1.x = __fadd_rn(s1.x, b1.x); s1.y = __fadd_rn(s1.y, b1.y); s1.z = __fadd_rn(s1.z, b1.z); s1.w = __fadd_rn(s1.w, b1.w);
+  // lane l combines warps for hypotheses (l >> 3) and (l >> 3) + 4; butterflies
+  // over the warp index (l & 7) give the lanes of a group identical totals
+  static_assert(NW == 8, "one lane per warp partial");
+  float x0 = red[buf][lane & 7][lane >> 3];
+  float x1 = red[buf][lane & 7][(lane >> 3) + 4];
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) {
+    x0 = __fadd_rn(x0, __shfl_xor_sync(0xffffffffu, x0, o));
+    x1 = __fadd_rn(x1, __shfl_xor_sync(0xffffffffu, x1, o));
   }
-  out[0] = s0.x; out[1] = s0.y; out[2] = s0.z; out[3] = s0.w;
-  out[4] = s1.x; out[5] = s1.y; out[6] = s1.z; out[7] = s1.w;
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    out[h] = __shfl_sync(0xffffffffu, x0, 8 * h);
+    out[h + 4] = __shfl_sync(0xffffffffu, x1, 8 * h);
+  }
   buf ^= 1;
 }
 
