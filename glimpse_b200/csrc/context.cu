@@ -444,7 +444,7 @@ int Context::run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
 // log-likelihood per haplotype into d_loglik.
 int Context::run_impute_ckpt(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
   ImputeWork& w = impute;
-  const int n = w.n;
+  const int n = w.n, L = w.L;
   const bool bf16 = precision_mode == GP_PRECISION_CKPT_BF16;
   cudaError_t e;
   if ((e = ckpt.ensure((size_t)n * w.WB * w.Kp * (bf16 ? 2 : 4))) != cudaSuccess) return cuda_fail(e, "alloc ckpt");

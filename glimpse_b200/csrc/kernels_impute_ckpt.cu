@@ -17,12 +17,16 @@
 //   * the log of every AlphaSum is accumulated in FP64: the chunk
 //     log-likelihood sum_l log AlphaSum_l (the reference keeps no such value).
 // With FP32 checkpoints the recomputed rows equal the first pass's bit for bit.
+// One CTA of 256 threads runs one haplotype; thread x owns states x + 256 j.
+// The per-site sums are block reductions in one fixed tree.
 #include <cuda_bf16.h>
 
 #include "internal.h"
 
 namespace gp {
 namespace {
+
+constexpr int kCT = 256, kCJ = kMaxStates / kCT, kCW = kCT / 32;
 
 struct CkptArgs {
   const int32_t* poly;
@@ -40,60 +44,77 @@ struct CkptArgs {
   double* loglik;   // [t] sum of log AlphaSum over the polymorphic sites
 };
 
-__device__ __forceinline__ float& comp4(float4& v, int c) { return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w; }
-__device__ __forceinline__ uint32_t comp4u(const uint4& v, int c) {
-  return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
-}
-// Two floats rounded to BF16 (the first in the low half, the lower address).
-__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
-  const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
-  return *reinterpret_cast<const uint32_t*>(&h);
-}
-__device__ __forceinline__ float bf16_lo(uint32_t u) { return __bfloat162float(__ushort_as_bfloat16((unsigned short)(u & 0xFFFFu))); }
-__device__ __forceinline__ float bf16_hi(uint32_t u) { return __bfloat162float(__ushort_as_bfloat16((unsigned short)(u >> 16))); }
-
-// One warp per haplotype, no block barriers: lane l owns the 4 J states
-// 128 j + 4 l + c (c = 0..3; states from K up are masked), so its entries of a
-// row are one aligned 16-byte vector; the per-site sums are warp butterflies in
-// a fixed order (over the lane's quads and components, then the lanes).
-constexpr int kCkWarps = 2;  // haplotypes (warps) per CTA
-
-__device__ __forceinline__ float warp_sum_ck(float v) {
+// Sums of N values over the CTA: warp butterflies, then the warps in one tree.
+// The partials alternate between two buffers, so one barrier per reduction
+// suffices: a reduction's writes go to the buffer that the previous one did
+// not read, and the one before that was read before the previous barrier.
+template <int N>
+__device__ __forceinline__ void cta_sum(float (&v)[N], float (*red)[3][kCW], int& buf) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = __fadd_rn(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
-  return v;
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[i] = __fadd_rn(v[i], __shfl_xor_sync(0xFFFFFFFFu, v[i], o));
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int i = 0; i < N; ++i) red[buf][i][threadIdx.x >> 5] = v[i];
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    const float* r = red[buf][i];
+    v[i] = __fadd_rn(__fadd_rn(__fadd_rn(r[0], r[1]), __fadd_rn(r[2], r[3])),
+                     __fadd_rn(__fadd_rn(r[4], r[5]), __fadd_rn(r[6], r[7])));
+  }
+  buf ^= 1;
 }
 
-template <int J, bool BF16>
-__global__ void __launch_bounds__(32 * kCkWarps) k_impute_ckpt_warp(CkptArgs a, int n) {
-  const int lane = threadIdx.x & 31;
-  const int t = blockIdx.x * kCkWarps + (threadIdx.x >> 5);
-  if (t >= n) return;
+template <bool BF16>
+__global__ void __launch_bounds__(kCT) k_impute_ckpt(CkptArgs a) {
+  static_assert(kCW == 8, "eight warps");
+  __shared__ float red[2][3][kCW];
+  int buf = 0;
+  const int t = blockIdx.x, tid = threadIdx.x;
   const int np = a.npoly[t], K = a.nstates[t];
   if (np <= 0 || K <= 0) return;
-  const int Kp = a.Kp;
-  const uint32_t* hv = a.hvar + (size_t)t * a.WB * Kp;
+  const uint32_t* hv = a.hvar + (size_t)t * a.WB * a.Kp;
   const float4* E = a.em + (size_t)t * a.L;
   const float2* TR = a.tr + (size_t)t * a.L;
   const uint8_t* F = a.fl + (size_t)t * a.L;
   const int32_t* PL = a.poly + (size_t)t * a.L;
   float* HP = a.hp + (size_t)t * 2 * a.L;
-  float* scr = a.scratch + (size_t)t * 32 * Kp;
+  float* scr = a.scratch + (size_t)t * 32 * a.Kp;
   float* cs = a.csum + (size_t)t * a.WB;
   const float invK = 1.0f / (float)K;
-  const int kb = 4 * lane;
-  // state k of (j, c) is kb + 128 j + c; quad j is held when kb + 128 j < Kp
-  auto held = [&](int j) { return kb + 128 * j < Kp; };
-  auto valid = [&](int j, int c) { return kb + 128 * j + c < K; };
-  uint4 w[J];
+  bool valid[kCJ];
+#pragma unroll
+  for (int j = 0; j < kCJ; ++j) valid[j] = tid + kCT * j < K;
+  uint32_t w[kCJ];
   auto load_words = [&](int blk) {
 #pragma unroll
-    for (int j = 0; j < J; ++j)
-      w[j] = held(j) ? *reinterpret_cast<const uint4*>(hv + (size_t)blk * Kp + kb + 128 * j) : make_uint4(0, 0, 0, 0);
+    for (int j = 0; j < kCJ; ++j) w[j] = valid[j] ? hv[(size_t)blk * a.Kp + tid + kCT * j] : 0u;
   };
-  auto ckpt_off = [&](int blk, int j) { return ((size_t)t * a.WB + blk) * Kp + kb + 128 * j; };
+  auto store_ckpt = [&](int blk, const float (&x)[kCJ]) {
+#pragma unroll
+    for (int j = 0; j < kCJ; ++j) {
+      if (!valid[j]) continue;
+      const size_t o = ((size_t)t * a.WB + blk) * a.Kp + tid + kCT * j;
+      if (BF16) reinterpret_cast<__nv_bfloat16*>(a.ckpt)[o] = __float2bfloat16_rn(x[j]);
+      else reinterpret_cast<float*>(a.ckpt)[o] = x[j];
+    }
+  };
+  auto load_ckpt = [&](int blk, float (&x)[kCJ]) {
+#pragma unroll
+    for (int j = 0; j < kCJ; ++j) {
+      if (!valid[j]) {
+        x[j] = 0.f;
+        continue;
+      }
+      const size_t o = ((size_t)t * a.WB + blk) * a.Kp + tid + kCT * j;
+      x[j] = BF16 ? __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(a.ckpt)[o])
+                  : reinterpret_cast<const float*>(a.ckpt)[o];
+    }
+  };
   // one forward step at site l from (x, acc) of site l - 1
-  auto fwd_step = [&](int l, float4 (&x)[J], float& acc) {
+  auto fwd_step = [&](int l, float (&x)[kCJ], float& acc) {
     const uint8_t f = F[l];
     const float4 e = E[l];
     const float ex = f ? 1.0f : e.x, ey = f ? 1.0f : e.y;
@@ -106,78 +127,57 @@ __global__ void __launch_bounds__(32 * kCkWarps) k_impute_ckpt_warp(CkptArgs a, 
       f2 = tp.y / acc;
     }
     const uint32_t m = 1u << (l & 31);
-    float s = 0.f;
+    float s[1] = {0.f};
 #pragma unroll
-    for (int j = 0; j < J; ++j) {
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const float xo = comp4(x[j], c);
-        const float pc = l == 0 ? f1 : fmaf(xo, f2, f1);
-        const float xn = valid(j, c) ? __fmul_rn(pc, (comp4u(w[j], c) & m) ? ey : ex) : 0.f;
-        comp4(x[j], c) = xn;
-        s = __fadd_rn(s, xn);
-      }
+    for (int j = 0; j < kCJ; ++j) {
+      const float pc = l == 0 ? f1 : fmaf(x[j], f2, f1);
+      x[j] = valid[j] ? __fmul_rn(pc, (w[j] & m) ? ey : ex) : 0.f;
+      s[0] = __fadd_rn(s[0], x[j]);
     }
-    s = warp_sum_ck(s);
-    acc = (l == 0 && f) ? 1.0f : s;  // AlphaSum = 1 at a flat first site (imputation_hmm.cpp:156)
+    cta_sum<1>(s, red, buf);
+    acc = (l == 0 && f) ? 1.0f : s[0];  // AlphaSum = 1 at a flat first site (imputation_hmm.cpp:156)
   };
 
   // ---- forward: checkpoints and the FP64 log-likelihood ----
-  float4 x[J];
-#pragma unroll
-  for (int j = 0; j < J; ++j) x[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+  float x[kCJ];
   float acc = 0.f;
   double ll = 0.0;
+#pragma unroll
+  for (int j = 0; j < kCJ; ++j) x[j] = 0.f;
   for (int l = 0; l < np; ++l) {
     if ((l & 31) == 0) load_words(l >> 5);
     fwd_step(l, x, acc);
-    if (lane == 0) ll += log((double)acc);
+    ll += log((double)acc);
     if ((l & 31) == 31 && l + 1 < np) {
-      const int blk = l >> 5;
-#pragma unroll
-      for (int j = 0; j < J; ++j) {
-        if (!held(j)) continue;
-        if (BF16) {
-          const uint32_t lo = pack_bf16x2(x[j].x, x[j].y), hi = pack_bf16x2(x[j].z, x[j].w);
-          *reinterpret_cast<uint2*>(reinterpret_cast<__nv_bfloat16*>(a.ckpt) + ckpt_off(blk, j)) = make_uint2(lo, hi);
-        } else {
-          *reinterpret_cast<float4*>(reinterpret_cast<float*>(a.ckpt) + ckpt_off(blk, j)) = x[j];
-        }
-      }
-      if (lane == 0) cs[blk] = acc;
+      store_ckpt(l >> 5, x);
+      if (tid == 0) cs[l >> 5] = acc;
     }
   }
-  if (lane == 0) a.loglik[t] = ll;
+  if (tid == 0) a.loglik[t] = ll;
 
   // ---- backward, block by block with the forward rows recomputed ----
-  float4 xb[J];
-#pragma unroll
-  for (int j = 0; j < J; ++j) xb[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+  float xb[kCJ];
   float bacc = 0.f;
+#pragma unroll
+  for (int j = 0; j < kCJ; ++j) xb[j] = 0.f;
   const int nblk = (np + 31) >> 5;
   for (int b = nblk - 1; b >= 0; --b) {
     const int s0 = b << 5, s1 = min(np, s0 + 32) - 1;
     load_words(b);
+    float xa[kCJ];
     float aacc = 0.f;
+    if (b > 0) {
+      load_ckpt(b - 1, xa);
+      aacc = cs[b - 1];
+    } else {
 #pragma unroll
-    for (int j = 0; j < J; ++j) {
-      x[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (b > 0 && held(j)) {
-        if (BF16) {
-          const uint2 u = *reinterpret_cast<const uint2*>(reinterpret_cast<const __nv_bfloat16*>(a.ckpt) +
-                                                         ckpt_off(b - 1, j));
-          x[j] = make_float4(bf16_lo(u.x), bf16_hi(u.x), bf16_lo(u.y), bf16_hi(u.y));
-        } else {
-          x[j] = *reinterpret_cast<const float4*>(reinterpret_cast<const float*>(a.ckpt) + ckpt_off(b - 1, j));
-        }
-      }
+      for (int j = 0; j < kCJ; ++j) xa[j] = 0.f;
     }
-    if (b > 0) aacc = cs[b - 1];
     for (int l = s0; l <= s1; ++l) {
-      fwd_step(l, x, aacc);
+      fwd_step(l, xa, aacc);
 #pragma unroll
-      for (int j = 0; j < J; ++j)
-        if (held(j)) *reinterpret_cast<float4*>(scr + (size_t)(l - s0) * Kp + kb + 128 * j) = x[j];
+      for (int j = 0; j < kCJ; ++j)
+        if (valid[j]) scr[(size_t)(l - s0) * a.Kp + tid + kCT * j] = xa[j];
     }
     for (int l = s1; l >= s0; --l) {
       const uint8_t f = F[l];
@@ -191,30 +191,22 @@ __global__ void __launch_bounds__(32 * kCkWarps) k_impute_ckpt_warp(CkptArgs a, 
         f2 = tt.y / bacc;
       }
       const uint32_t m = 1u << (l & 31);
-      float v0 = 0.f, v1 = 0.f, v2 = 0.f;  // betaSum, prob_hid 0, prob_hid 1
+      float v[3] = {0.f, 0.f, 0.f};  // betaSum, prob_hid 0, prob_hid 1
 #pragma unroll
-      for (int j = 0; j < J; ++j) {
-        float4 al = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (held(j)) al = *reinterpret_cast<const float4*>(scr + (size_t)(l - s0) * Kp + kb + 128 * j);
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          if (!valid(j, c)) continue;
-          const bool bit = (comp4u(w[j], c) & m) != 0u;
-          const float pc = last ? f1 : fmaf(comp4(xb[j], c), f2, f1);
-          const float ac = comp4(al, c);
-          const float d = last ? ac : __fmul_rn(ac, pc);  // alpha alone at the last site
-          if (bit) v2 = __fadd_rn(v2, d);
-          else v1 = __fadd_rn(v1, d);
-          const float xn = __fmul_rn(pc, bit ? ey : ex);
-          comp4(xb[j], c) = xn;
-          v0 = __fadd_rn(v0, xn);
-        }
+      for (int j = 0; j < kCJ; ++j) {
+        if (!valid[j]) continue;
+        const bool bit = (w[j] & m) != 0u;
+        const float al = scr[(size_t)(l - s0) * a.Kp + tid + kCT * j];
+        const float pc = last ? f1 : fmaf(xb[j], f2, f1);
+        const float d = last ? al : __fmul_rn(al, pc);  // alpha alone at the last site
+        if (bit) v[2] = __fadd_rn(v[2], d);
+        else v[1] = __fadd_rn(v[1], d);
+        xb[j] = __fmul_rn(pc, bit ? ey : ex);
+        v[0] = __fadd_rn(v[0], xb[j]);
       }
-      v0 = warp_sum_ck(v0);
-      v1 = warp_sum_ck(v1);
-      v2 = warp_sum_ck(v2);
-      bacc = (last && f) ? 1.0f : v0;  // betaSum = 1 at a flat last site (imputation_hmm.cpp:285)
-      if (lane == 0) *reinterpret_cast<float2*>(HP + 2 * PL[l]) = make_float2(v1, v2);
+      cta_sum<3>(v, red, buf);
+      bacc = (last && f) ? 1.0f : v[0];  // betaSum = 1 at a flat last site (imputation_hmm.cpp:285)
+      if (tid == 0) *reinterpret_cast<float2*>(HP + 2 * PL[l]) = make_float2(v[1], v[2]);
     }
   }
 }
@@ -240,23 +232,8 @@ int launch_impute_ckpt(ImputeWork& w, bool bf16, void* ckpt, float* csum, float*
   a.hp = hp;
   a.loglik = loglik;
   if (w.Kp > kMaxStates) return GP_E_ARG;
-  // quads per lane: the smallest instantiated J with 128 J >= Kp
-  const int jn = (w.Kp + 127) / 128;
-  const int grid = (w.n + kCkWarps - 1) / kCkWarps;
-#define GP_CK_LAUNCH(JJ)                                                                     \
-  if (jn <= JJ) {                                                                            \
-    if (bf16) k_impute_ckpt_warp<JJ, true><<<grid, 32 * kCkWarps, 0, s>>>(a, w.n);            \
-    else k_impute_ckpt_warp<JJ, false><<<grid, 32 * kCkWarps, 0, s>>>(a, w.n);                \
-    return GP_OK;                                                                            \
-  }
-  GP_CK_LAUNCH(2)
-  GP_CK_LAUNCH(4)
-  GP_CK_LAUNCH(6)
-  GP_CK_LAUNCH(8)
-  GP_CK_LAUNCH(10)
-  GP_CK_LAUNCH(12)
-  GP_CK_LAUNCH(16)
-#undef GP_CK_LAUNCH
+  if (bf16) k_impute_ckpt<true><<<w.n, kCT, 0, s>>>(a);
+  else k_impute_ckpt<false><<<w.n, kCT, 0, s>>>(a);
   return GP_OK;
 }
 
