@@ -444,13 +444,15 @@ int Context::run_impute(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
 // log-likelihood per haplotype into d_loglik.
 int Context::run_impute_ckpt(const float* d_hl, const uint8_t* d_flat, float* d_hp) {
   ImputeWork& w = impute;
-  const int n = w.n, L = w.L;
+  const int n = w.n;
   const bool bf16 = precision_mode == GP_PRECISION_CKPT_BF16;
   cudaError_t e;
-  if ((e = ckpt.ensure((size_t)n * w.WB * w.Kp * (bf16 ? 2 : 4))) != cudaSuccess) return cuda_fail(e, "alloc ckpt");
-  if ((e = ckpt_sum.ensure((size_t)n * w.WB * 4)) != cudaSuccess) return cuda_fail(e, "alloc ckpt");
-  if ((e = ckpt_scratch.ensure((size_t)n * 32 * w.Kp * 4)) != cudaSuccess) return cuda_fail(e, "alloc ckpt");
-  if ((e = loglik.ensure((size_t)n * 8)) != cudaSuccess) return cuda_fail(e, "alloc loglik");
+  // alpha and beta checkpoints and their sums, one 32-row scratch per chain,
+  // the log-likelihood and its first half
+  if ((e = ckpt.ensure((size_t)2 * n * w.WB * w.Kp * (bf16 ? 2 : 4))) != cudaSuccess) return cuda_fail(e, "alloc ckpt");
+  if ((e = ckpt_sum.ensure((size_t)2 * n * w.WB * 4)) != cudaSuccess) return cuda_fail(e, "alloc ckpt");
+  if ((e = ckpt_scratch.ensure((size_t)2 * n * 32 * w.Kp * 4)) != cudaSuccess) return cuda_fail(e, "alloc ckpt");
+  if ((e = loglik.ensure((size_t)2 * n * 8)) != cudaSuccess) return cuda_fail(e, "alloc loglik");
   launch_site_records(panel, mc, w, d_hl, d_flat, stream);
   double cells = 0;
   for (int i = 0; i < n; ++i) cells += (double)impute_np[i] * (double)host_nstates[i];
@@ -461,7 +463,7 @@ int Context::run_impute_ckpt(const float* d_hl, const uint8_t* d_flat, float* d_
     return (fail(GP_E_ARG, "imputation: too many states"), GP_E_ARG);
   prof_end(ea, 0, cells);
   launch_impute_finish(panel, mc, w, d_hl, d_flat, d_hp, stream);
-  prof.kernel_launches += 3;
+  prof.kernel_launches += 4;
   loglik_n = n;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "imputation launch");
   return GP_OK;

@@ -1,24 +1,33 @@
 // The precision variant of the imputation forward-backward: checkpointed
-// forward messages with recompute, and an FP64 chunk log-likelihood.
+// messages with recompute, and an FP64 chunk log-likelihood.
 //
 // Same HMM and same per-site arithmetic as the full-store chains
 // (kernels_impute_warp.cu, after imputation_hmm.cpp:80-353): forward
 // alpha_l = (alpha_{l-1} (1 - t) / AlphaSum_{l-1} + t / K) e_l, backward
 // beta likewise with betaSum, prob_hid of each allele = sum over states of
-// alpha_l x (backward message before the emission at l). What differs is what
-// is kept between the passes:
-//   * the forward pass keeps only the row after the last site of every block of
-//     32 polymorphic sites (FP32, or BF16 for the lower-memory variant), with
-//     that site's AlphaSum in FP32;
-//   * the backward pass walks the blocks from the last to the first; for each
-//     it recomputes the block's 32 forward rows in FP32 from the previous
-//     block's checkpoint into a per-haplotype scratch of 32 rows (it stays in
-//     L2), then runs the backward steps over the block reading them;
-//   * the log of every AlphaSum is accumulated in FP64: the chunk
-//     log-likelihood sum_l log AlphaSum_l (the reference keeps no such value).
-// With FP32 checkpoints the recomputed rows equal the first pass's bit for bit.
-// One CTA of 256 threads runs one haplotype; thread x owns states x + 256 j.
-// The per-site sums are block reductions in one fixed tree.
+// alpha_l x (backward message before the emission at l, 1 at the last site).
+// What differs is what is kept between the passes. As in the full-store
+// chains, each haplotype is split at M (a multiple of 32, about np / 2) into a
+// forward and a backward chain that run concurrently, one CTA each:
+//   phase A  forward  [0, M)      keeps the alpha row after the last site of
+//                                 every block of 32 polymorphic sites, and its
+//                                 AlphaSum
+//            backward [np-1, M]   keeps the beta row after the first site of
+//                                 every block, and its betaSum
+//   phase B  forward  [M, np)     per block: the block's backward messages are
+//                                 recomputed from the next block's checkpoint
+//                                 into a 32-row scratch, then the forward steps
+//                                 form the posteriors from them
+//            backward [M-1, 0]    per block: the block's alpha rows are
+//                                 recomputed from the previous block's
+//                                 checkpoint into the scratch, then the
+//                                 backward steps form the posteriors
+// Checkpoints are FP32, or BF16 for the lower-memory variant; recomputed rows
+// are FP32 (with FP32 checkpoints they equal the first pass's bit for bit).
+// The log of every AlphaSum is accumulated in FP64: the chunk log-likelihood
+// sum_l log AlphaSum_l (the reference keeps no such value).
+// One CTA of 256 threads runs one chain; thread x owns states x + 256 j. The
+// per-site sums are block reductions in one fixed tree.
 #include <cuda_bf16.h>
 
 #include "internal.h"
@@ -36,12 +45,13 @@ struct CkptArgs {
   const float4* em;
   const float2* tr;
   const uint8_t* fl;
-  int L, WB, Kp;
-  void* ckpt;       // [t][WB][Kp] rows after each block's last site (float or BF16)
-  float* csum;      // [t][WB] AlphaSum at those sites
-  float* scratch;   // [t][32][Kp] the recomputed rows of one block
+  int n, L, WB, Kp;
+  void* ckpt;       // [2][t][WB][Kp]: alpha after each block's last site, beta after its first (float or BF16)
+  float* csum;      // [2][t][WB]: AlphaSum / betaSum at those sites
+  float* scratch;   // [t][2][32][Kp]: the recomputed rows of one block, per chain
   float* hp;        // [t][2L]: (prob_hid 0, prob_hid 1) at each polymorphic site
-  double* loglik;   // [t] sum of log AlphaSum over the polymorphic sites
+  double* llpart;   // [t]: sum of log AlphaSum over [0, M)
+  double* loglik;   // [t]: sum of log AlphaSum over the polymorphic sites
 };
 
 // Sums of N values over the CTA: warp butterflies, then the warps in one tree.
@@ -67,22 +77,28 @@ __device__ __forceinline__ void cta_sum(float (&v)[N], float (*red)[3][kCW], int
   buf ^= 1;
 }
 
-template <bool BF16>
+// M of the meet-in-the-middle split (as the full-store chains take it).
+__device__ __forceinline__ int ckpt_split(int np) { return (np / 2) & ~31; }
+
+// Phase A (PB = false) or phase B (PB = true) of one chain: CTA 2 t + role runs
+// haplotype t's forward (role 0) or backward (role 1) chain.
+template <bool BF16, bool PB>
 __global__ void __launch_bounds__(kCT) k_impute_ckpt(CkptArgs a) {
   static_assert(kCW == 8, "eight warps");
   __shared__ float red[2][3][kCW];
   int buf = 0;
-  const int t = blockIdx.x, tid = threadIdx.x;
+  const int t = blockIdx.x >> 1, role = blockIdx.x & 1, tid = threadIdx.x;
   const int np = a.npoly[t], K = a.nstates[t];
   if (np <= 0 || K <= 0) return;
-  const uint32_t* hv = a.hvar + (size_t)t * a.WB * a.Kp;
+  const int M = ckpt_split(np);
+  const int Kp = a.Kp;
+  const uint32_t* hv = a.hvar + (size_t)t * a.WB * Kp;
   const float4* E = a.em + (size_t)t * a.L;
   const float2* TR = a.tr + (size_t)t * a.L;
   const uint8_t* F = a.fl + (size_t)t * a.L;
   const int32_t* PL = a.poly + (size_t)t * a.L;
   float* HP = a.hp + (size_t)t * 2 * a.L;
-  float* scr = a.scratch + (size_t)t * 32 * a.Kp;
-  float* cs = a.csum + (size_t)t * a.WB;
+  float* scr = a.scratch + ((size_t)t * 2 + role) * 32 * Kp;
   const float invK = 1.0f / (float)K;
   bool valid[kCJ];
 #pragma unroll
@@ -90,27 +106,28 @@ __global__ void __launch_bounds__(kCT) k_impute_ckpt(CkptArgs a) {
   uint32_t w[kCJ];
   auto load_words = [&](int blk) {
 #pragma unroll
-    for (int j = 0; j < kCJ; ++j) w[j] = valid[j] ? hv[(size_t)blk * a.Kp + tid + kCT * j] : 0u;
+    for (int j = 0; j < kCJ; ++j) w[j] = valid[j] ? hv[(size_t)blk * Kp + tid + kCT * j] : 0u;
   };
-  auto store_ckpt = [&](int blk, const float (&x)[kCJ]) {
+  // checkpoint d (0 alpha, 1 beta) of block blk
+  auto row_off = [&](int d, int blk, int j) {
+    return (((size_t)d * a.n + t) * a.WB + blk) * Kp + tid + kCT * j;
+  };
+  auto sum_off = [&](int d, int blk) { return ((size_t)d * a.n + t) * a.WB + blk; };
+  auto store_row = [&](int d, int blk, const float (&x)[kCJ]) {
 #pragma unroll
     for (int j = 0; j < kCJ; ++j) {
       if (!valid[j]) continue;
-      const size_t o = ((size_t)t * a.WB + blk) * a.Kp + tid + kCT * j;
-      if (BF16) reinterpret_cast<__nv_bfloat16*>(a.ckpt)[o] = __float2bfloat16_rn(x[j]);
-      else reinterpret_cast<float*>(a.ckpt)[o] = x[j];
+      if (BF16) reinterpret_cast<__nv_bfloat16*>(a.ckpt)[row_off(d, blk, j)] = __float2bfloat16_rn(x[j]);
+      else reinterpret_cast<float*>(a.ckpt)[row_off(d, blk, j)] = x[j];
     }
   };
-  auto load_ckpt = [&](int blk, float (&x)[kCJ]) {
+  auto load_row = [&](int d, int blk, float (&x)[kCJ]) {
 #pragma unroll
     for (int j = 0; j < kCJ; ++j) {
-      if (!valid[j]) {
-        x[j] = 0.f;
-        continue;
-      }
-      const size_t o = ((size_t)t * a.WB + blk) * a.Kp + tid + kCT * j;
-      x[j] = BF16 ? __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(a.ckpt)[o])
-                  : reinterpret_cast<const float*>(a.ckpt)[o];
+      x[j] = 0.f;
+      if (!valid[j]) continue;
+      x[j] = BF16 ? __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(a.ckpt)[row_off(d, blk, j)])
+                  : reinterpret_cast<const float*>(a.ckpt)[row_off(d, blk, j)];
     }
   };
   // one forward step at site l from (x, acc) of site l - 1
@@ -137,76 +154,182 @@ __global__ void __launch_bounds__(kCT) k_impute_ckpt(CkptArgs a) {
     cta_sum<1>(s, red, buf);
     acc = (l == 0 && f) ? 1.0f : s[0];  // AlphaSum = 1 at a flat first site (imputation_hmm.cpp:156)
   };
-
-  // ---- forward: checkpoints and the FP64 log-likelihood ----
-  float x[kCJ];
-  float acc = 0.f;
-  double ll = 0.0;
-#pragma unroll
-  for (int j = 0; j < kCJ; ++j) x[j] = 0.f;
-  for (int l = 0; l < np; ++l) {
-    if ((l & 31) == 0) load_words(l >> 5);
-    fwd_step(l, x, acc);
-    ll += log((double)acc);
-    if ((l & 31) == 31 && l + 1 < np) {
-      store_ckpt(l >> 5, x);
-      if (tid == 0) cs[l >> 5] = acc;
+  // one backward step at site l from (xb, bacc) of site l + 1; pc gets the
+  // message before the emission at l (1 at the last site), as the full store keeps it
+  auto bwd_step = [&](int l, float (&xb)[kCJ], float& bacc, float (&pc)[kCJ]) {
+    const uint8_t f = F[l];
+    const float4 e = E[l];
+    const float ex = f ? 1.0f : e.x, ey = f ? 1.0f : e.y;
+    const bool last = l == np - 1;
+    float f1 = invK, f2 = 0.f;
+    if (!last) {
+      const float2 tt = TR[l];
+      f1 = tt.x;
+      f2 = tt.y / bacc;
     }
-  }
-  if (tid == 0) a.loglik[t] = ll;
-
-  // ---- backward, block by block with the forward rows recomputed ----
-  float xb[kCJ];
-  float bacc = 0.f;
+    const uint32_t m = 1u << (l & 31);
+    float s[1] = {0.f};
 #pragma unroll
-  for (int j = 0; j < kCJ; ++j) xb[j] = 0.f;
+    for (int j = 0; j < kCJ; ++j) {
+      pc[j] = 0.f;
+      if (!valid[j]) continue;
+      const float p = last ? f1 : fmaf(xb[j], f2, f1);
+      pc[j] = last ? 1.0f : p;
+      xb[j] = __fmul_rn(p, (w[j] & m) ? ey : ex);
+      s[0] = __fadd_rn(s[0], xb[j]);
+    }
+    cta_sum<1>(s, red, buf);
+    bacc = (last && f) ? 1.0f : s[0];  // betaSum = 1 at a flat last site (imputation_hmm.cpp:285)
+  };
+
+  float x[kCJ], pc[kCJ];
+  if (!PB) {
+    if (role == 0) {
+      // ---- phase A forward over [0, M): alpha checkpoints, log-likelihood ----
+      if (M == 0) return;
+      float acc = 0.f;
+      double ll = 0.0;
+#pragma unroll
+      for (int j = 0; j < kCJ; ++j) x[j] = 0.f;
+      for (int l = 0; l < M; ++l) {
+        if ((l & 31) == 0) load_words(l >> 5);
+        fwd_step(l, x, acc);
+        ll += log((double)acc);
+        if ((l & 31) == 31) {
+          store_row(0, l >> 5, x);
+          if (tid == 0) a.csum[sum_off(0, l >> 5)] = acc;
+        }
+      }
+      if (tid == 0) a.llpart[t] = ll;
+    } else {
+      // ---- phase A backward over [np-1, M]: beta checkpoints ----
+      float bacc = 0.f;
+#pragma unroll
+      for (int j = 0; j < kCJ; ++j) x[j] = 0.f;
+      for (int l = np - 1; l >= M; --l) {
+        if (l == np - 1 || (l & 31) == 31) load_words(l >> 5);
+        bwd_step(l, x, bacc, pc);
+        if ((l & 31) == 0) {
+          store_row(1, l >> 5, x);
+          if (tid == 0) a.csum[sum_off(1, l >> 5)] = bacc;
+        }
+      }
+    }
+    return;
+  }
+
   const int nblk = (np + 31) >> 5;
-  for (int b = nblk - 1; b >= 0; --b) {
-    const int s0 = b << 5, s1 = min(np, s0 + 32) - 1;
-    load_words(b);
-    float xa[kCJ];
-    float aacc = 0.f;
-    if (b > 0) {
-      load_ckpt(b - 1, xa);
-      aacc = cs[b - 1];
+  if (role == 0) {
+    // ---- phase B forward over [M, np): per block, the backward messages
+    // recomputed from the next block's checkpoint, then alpha and the posteriors ----
+    float acc = 0.f;
+    double ll = 0.0;
+    if (M > 0) {
+      load_row(0, (M >> 5) - 1, x);
+      acc = a.csum[sum_off(0, (M >> 5) - 1)];
+      ll = a.llpart[t];
     } else {
 #pragma unroll
-      for (int j = 0; j < kCJ; ++j) xa[j] = 0.f;
+      for (int j = 0; j < kCJ; ++j) x[j] = 0.f;
     }
-    for (int l = s0; l <= s1; ++l) {
-      fwd_step(l, xa, aacc);
+    for (int b = M >> 5; b < nblk; ++b) {
+      const int s0 = b << 5, s1 = min(np, s0 + 32) - 1;
+      load_words(b);
+      float xb[kCJ];
+      float bacc = 0.f;
+      if (b + 1 < nblk) {
+        load_row(1, b + 1, xb);
+        bacc = a.csum[sum_off(1, b + 1)];
+      } else {
 #pragma unroll
-      for (int j = 0; j < kCJ; ++j)
-        if (valid[j]) scr[(size_t)(l - s0) * a.Kp + tid + kCT * j] = xa[j];
+        for (int j = 0; j < kCJ; ++j) xb[j] = 0.f;
+      }
+      for (int l = s1; l >= s0; --l) {
+        bwd_step(l, xb, bacc, pc);
+#pragma unroll
+        for (int j = 0; j < kCJ; ++j)
+          if (valid[j]) scr[(size_t)(l - s0) * Kp + tid + kCT * j] = pc[j];
+      }
+      for (int l = s0; l <= s1; ++l) {
+        const uint8_t f = F[l];
+        const float4 e = E[l];
+        const float ex = f ? 1.0f : e.x, ey = f ? 1.0f : e.y;
+        float f1, f2 = 0.f;
+        if (l == 0) {
+          f1 = invK;
+        } else {
+          const float2 tp = TR[l - 1];
+          f1 = tp.x;
+          f2 = tp.y / acc;
+        }
+        const uint32_t m = 1u << (l & 31);
+        float v[3] = {0.f, 0.f, 0.f};  // AlphaSum, prob_hid 0, prob_hid 1
+#pragma unroll
+        for (int j = 0; j < kCJ; ++j) {
+          const float p = l == 0 ? f1 : fmaf(x[j], f2, f1);
+          const bool bit = (w[j] & m) != 0u;
+          x[j] = valid[j] ? __fmul_rn(p, bit ? ey : ex) : 0.f;
+          v[0] = __fadd_rn(v[0], x[j]);
+          if (!valid[j]) continue;
+          const float d = __fmul_rn(x[j], scr[(size_t)(l - s0) * Kp + tid + kCT * j]);  // alpha x message (1 at the last site)
+          if (bit) v[2] = __fadd_rn(v[2], d);
+          else v[1] = __fadd_rn(v[1], d);
+        }
+        cta_sum<3>(v, red, buf);
+        acc = (l == 0 && f) ? 1.0f : v[0];  // AlphaSum = 1 at a flat first site (imputation_hmm.cpp:156)
+        ll += log((double)acc);
+        if (tid == 0) *reinterpret_cast<float2*>(HP + 2 * PL[l]) = make_float2(v[1], v[2]);
+      }
     }
-    for (int l = s1; l >= s0; --l) {
-      const uint8_t f = F[l];
-      const float4 e = E[l];
-      const float ex = f ? 1.0f : e.x, ey = f ? 1.0f : e.y;
-      const bool last = l == np - 1;
-      float f1 = invK, f2 = 0.f;
-      if (!last) {
+    if (tid == 0) a.loglik[t] = ll;
+  } else {
+    // ---- phase B backward over [M-1, 0]: per block, the alpha rows recomputed
+    // from the previous block's checkpoint, then beta and the posteriors ----
+    if (M == 0) return;
+    float xb[kCJ];
+    load_row(1, M >> 5, xb);
+    float bacc = a.csum[sum_off(1, M >> 5)];
+    for (int b = (M >> 5) - 1; b >= 0; --b) {
+      const int s0 = b << 5, s1 = s0 + 31;
+      load_words(b);
+      float aacc = 0.f;
+      if (b > 0) {
+        load_row(0, b - 1, x);
+        aacc = a.csum[sum_off(0, b - 1)];
+      } else {
+#pragma unroll
+        for (int j = 0; j < kCJ; ++j) x[j] = 0.f;
+      }
+      for (int l = s0; l <= s1; ++l) {
+        fwd_step(l, x, aacc);
+#pragma unroll
+        for (int j = 0; j < kCJ; ++j)
+          if (valid[j]) scr[(size_t)(l - s0) * Kp + tid + kCT * j] = x[j];
+      }
+      for (int l = s1; l >= s0; --l) {  // l < M <= np - 1: never the last site
+        const uint8_t f = F[l];
+        const float4 e = E[l];
+        const float ex = f ? 1.0f : e.x, ey = f ? 1.0f : e.y;
         const float2 tt = TR[l];
-        f1 = tt.x;
-        f2 = tt.y / bacc;
-      }
-      const uint32_t m = 1u << (l & 31);
-      float v[3] = {0.f, 0.f, 0.f};  // betaSum, prob_hid 0, prob_hid 1
+        const float f1 = tt.x, f2 = tt.y / bacc;
+        const uint32_t m = 1u << (l & 31);
+        float v[3] = {0.f, 0.f, 0.f};  // betaSum, prob_hid 0, prob_hid 1
 #pragma unroll
-      for (int j = 0; j < kCJ; ++j) {
-        if (!valid[j]) continue;
-        const bool bit = (w[j] & m) != 0u;
-        const float al = scr[(size_t)(l - s0) * a.Kp + tid + kCT * j];
-        const float pc = last ? f1 : fmaf(xb[j], f2, f1);
-        const float d = last ? al : __fmul_rn(al, pc);  // alpha alone at the last site
-        if (bit) v[2] = __fadd_rn(v[2], d);
-        else v[1] = __fadd_rn(v[1], d);
-        xb[j] = __fmul_rn(pc, bit ? ey : ex);
-        v[0] = __fadd_rn(v[0], xb[j]);
+        for (int j = 0; j < kCJ; ++j) {
+          if (!valid[j]) continue;
+          const bool bit = (w[j] & m) != 0u;
+          const float al = scr[(size_t)(l - s0) * Kp + tid + kCT * j];
+          const float p = fmaf(xb[j], f2, f1);
+          const float d = __fmul_rn(al, p);
+          if (bit) v[2] = __fadd_rn(v[2], d);
+          else v[1] = __fadd_rn(v[1], d);
+          xb[j] = __fmul_rn(p, bit ? ey : ex);
+          v[0] = __fadd_rn(v[0], xb[j]);
+        }
+        cta_sum<3>(v, red, buf);
+        bacc = v[0];
+        if (tid == 0) *reinterpret_cast<float2*>(HP + 2 * PL[l]) = make_float2(v[1], v[2]);
       }
-      cta_sum<3>(v, red, buf);
-      bacc = (last && f) ? 1.0f : v[0];  // betaSum = 1 at a flat last site (imputation_hmm.cpp:285)
-      if (tid == 0) *reinterpret_cast<float2*>(HP + 2 * PL[l]) = make_float2(v[1], v[2]);
     }
   }
 }
@@ -223,6 +346,7 @@ int launch_impute_ckpt(ImputeWork& w, bool bf16, void* ckpt, float* csum, float*
   a.em = w.em.as<float4>();
   a.tr = w.tr.as<float2>();
   a.fl = w.fl.as<uint8_t>();
+  a.n = w.n;
   a.L = w.L;
   a.WB = w.WB;
   a.Kp = w.Kp;
@@ -231,9 +355,16 @@ int launch_impute_ckpt(ImputeWork& w, bool bf16, void* ckpt, float* csum, float*
   a.scratch = scratch;
   a.hp = hp;
   a.loglik = loglik;
+  a.llpart = loglik + w.n;
   if (w.Kp > kMaxStates) return GP_E_ARG;
-  if (bf16) k_impute_ckpt<true><<<w.n, kCT, 0, s>>>(a);
-  else k_impute_ckpt<false><<<w.n, kCT, 0, s>>>(a);
+  const int grid = 2 * w.n;
+  if (bf16) {
+    k_impute_ckpt<true, false><<<grid, kCT, 0, s>>>(a);
+    k_impute_ckpt<true, true><<<grid, kCT, 0, s>>>(a);
+  } else {
+    k_impute_ckpt<false, false><<<grid, kCT, 0, s>>>(a);
+    k_impute_ckpt<false, true><<<grid, kCT, 0, s>>>(a);
+  }
   return GP_OK;
 }
 
