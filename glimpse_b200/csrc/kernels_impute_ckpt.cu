@@ -35,7 +35,7 @@
 namespace gp {
 namespace {
 
-constexpr int kCT = 256, kCJ = kMaxStates / kCT, kCW = kCT / 32;
+constexpr int kCT = 256, kCW = kCT / 32;
 
 struct CkptArgs {
   const int32_t* poly;
@@ -81,9 +81,11 @@ __device__ __forceinline__ void cta_sum(float (&v)[N], float (*red)[3][kCW], int
 __device__ __forceinline__ int ckpt_split(int np) { return (np / 2) & ~31; }
 
 // Phase A (PB = false) or phase B (PB = true) of one chain: CTA 2 t + role runs
-// haplotype t's forward (role 0) or backward (role 1) chain.
-template <bool BF16, bool PB>
+// haplotype t's forward (role 0) or backward (role 1) chain. J: states per
+// thread, from the launch's largest K.
+template <int J, bool BF16, bool PB>
 __global__ void __launch_bounds__(kCT) k_impute_ckpt(CkptArgs a) {
+  constexpr int kCJ = J;
   static_assert(kCW == 8, "eight warps");
   __shared__ float red[2][3][kCW];
   int buf = 0;
@@ -358,13 +360,25 @@ int launch_impute_ckpt(ImputeWork& w, bool bf16, void* ckpt, float* csum, float*
   a.llpart = loglik + w.n;
   if (w.Kp > kMaxStates) return GP_E_ARG;
   const int grid = 2 * w.n;
-  if (bf16) {
-    k_impute_ckpt<true, false><<<grid, kCT, 0, s>>>(a);
-    k_impute_ckpt<true, true><<<grid, kCT, 0, s>>>(a);
-  } else {
-    k_impute_ckpt<false, false><<<grid, kCT, 0, s>>>(a);
-    k_impute_ckpt<false, true><<<grid, kCT, 0, s>>>(a);
+  const int jn = (w.Kp + kCT - 1) / kCT;  // states per thread; the smallest instantiated J >= jn
+#define GP_CK_LAUNCH(JJ)                                         \
+  if (jn <= JJ) {                                                \
+    if (bf16) {                                                  \
+      k_impute_ckpt<JJ, true, false><<<grid, kCT, 0, s>>>(a);    \
+      k_impute_ckpt<JJ, true, true><<<grid, kCT, 0, s>>>(a);     \
+    } else {                                                     \
+      k_impute_ckpt<JJ, false, false><<<grid, kCT, 0, s>>>(a);   \
+      k_impute_ckpt<JJ, false, true><<<grid, kCT, 0, s>>>(a);    \
+    }                                                            \
+    return GP_OK;                                                \
   }
+  GP_CK_LAUNCH(2)
+  GP_CK_LAUNCH(3)
+  GP_CK_LAUNCH(4)
+  GP_CK_LAUNCH(5)
+  GP_CK_LAUNCH(6)
+  GP_CK_LAUNCH(8)
+#undef GP_CK_LAUNCH
   return GP_OK;
 }
 
