@@ -104,3 +104,35 @@ def test_state_list_arguments(small_workload):
             ctx.iteration(native.STAGE_INIT, 0)
     finally:
         ctx.close()
+
+
+@pytest.mark.gpu
+def test_state_lists_join_the_learned_selection():
+    """With the learned proposal on, the lists still join every set: each set
+    is the proposal's choice (at most the target's K) plus the target's rows,
+    sorted and without duplicates."""
+    from glimpse_b200 import native, synth
+    w = synth.make_panel_and_targets(2000, 12000, 1.5, 0.6, 6, ("uniform", 0.5, 2.0), ("fixed", 120), seed=33,
+                                     sparse_maf=0.005)
+    P, T = w.panel, w.targets
+    ctx = native.Context(P, kinit=300, kpbwt=120, pbwt_depth=8, pbwt_modulo_cm=0.05)
+    try:
+        ctx.set_targets(T, kpbwt=T.kpbwt)
+        lists = _lists(P.n_ref_haps, T.ploidy, 9, lo=5, hi=30)
+        ctx.set_state_lists(lists)
+        ctx.iteration(native.STAGE_INIT, 0)
+        ctx.iteration(native.STAGE_BURN, 1)
+        ctx.learned_train(kcand=512, kpos=8.0, steps=40, batch=4096, lr=1e-3, seed=3)
+        ctx.learned_enable(True, kcand=512)
+        ctx.iteration(native.STAGE_BURN, 2)
+        first = np.concatenate([[0], np.cumsum(T.ploidy)])
+        for t in range(T.n):
+            s = ctx.states(t).astype(np.int64)
+            rows = np.unique(np.concatenate(lists[first[t]:first[t + 1]]))
+            assert np.all(np.diff(s) > 0)
+            assert np.isin(rows, s).all()
+            assert s.size <= int(T.kpbwt[t]) + rows.size
+        h0, h1 = ctx.haps()
+        assert h0.shape == (T.n, P.n_sites)
+    finally:
+        ctx.close()
