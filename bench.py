@@ -509,6 +509,8 @@ def run_case(args):
         w = synth.workload(args.config, seed=1, n_targets=args.targets)
         T = w.targets
         ctx = native.Context(w.panel, kinit=w.params["kinit"], kpbwt=int(T.kpbwt.max()))
+        ctx.set_precision({"full": native.PRECISION_FULL, "f32": native.PRECISION_CKPT_F32,
+                           "bf16": native.PRECISION_CKPT_BF16}[args.precision])
         ctx.set_targets(T, kpbwt=T.kpbwt)
         for it in range(args.iterations):
             t0 = time.perf_counter()
