@@ -70,9 +70,9 @@ __device__ __forceinline__ void cta_sum(float (&v)[N], float (*red)[3][kCW], int
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < N; ++i) {
-    const float* r = red[buf][i];
-    v[i] = __fadd_rn(__fadd_rn(__fadd_rn(r[0], r[1]), __fadd_rn(r[2], r[3])),
-                     __fadd_rn(__fadd_rn(r[4], r[5]), __fadd_rn(r[6], r[7])));
+    const float4 p = reinterpret_cast<const float4*>(red[buf][i])[0], q = reinterpret_cast<const float4*>(red[buf][i])[1];
+    v[i] = __fadd_rn(__fadd_rn(__fadd_rn(p.x, p.y), __fadd_rn(p.z, p.w)),
+                     __fadd_rn(__fadd_rn(q.x, q.y), __fadd_rn(q.z, q.w)));
   }
   buf ^= 1;
 }
@@ -87,7 +87,7 @@ template <int J, bool BF16, bool PB>
 __global__ void __launch_bounds__(kCT) k_impute_ckpt(CkptArgs a) {
   constexpr int kCJ = J;
   static_assert(kCW == 8, "eight warps");
-  __shared__ float red[2][3][kCW];
+  __shared__ __align__(16) float red[2][3][kCW];  // rows of 8 partials read as two float4
   int buf = 0;
   const int t = blockIdx.x >> 1, role = blockIdx.x & 1, tid = threadIdx.x;
   const int np = a.npoly[t], K = a.nstates[t];
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(kCT) k_impute_ckpt(CkptArgs a) {
       for (int l = 0; l < M; ++l) {
         if ((l & 31) == 0) load_words(l >> 5);
         fwd_step(l, x, acc);
-        ll += log((double)acc);
+        if (tid == 0) ll += log((double)acc);  // thread 0 alone keeps the FP64 sum
         if ((l & 31) == 31) {
           store_row(0, l >> 5, x);
           if (tid == 0) a.csum[sum_off(0, l >> 5)] = acc;
@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(kCT) k_impute_ckpt(CkptArgs a) {
         }
         cta_sum<3>(v, red, buf);
         acc = (l == 0 && f) ? 1.0f : v[0];  // AlphaSum = 1 at a flat first site (imputation_hmm.cpp:156)
-        ll += log((double)acc);
+        if (tid == 0) ll += log((double)acc);  // thread 0 alone keeps the FP64 sum
         if (tid == 0) *reinterpret_cast<float2*>(HP + 2 * PL[l]) = make_float2(v[1], v[2]);
       }
     }
