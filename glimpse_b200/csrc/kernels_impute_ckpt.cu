@@ -105,9 +105,6 @@ __global__ void __launch_bounds__(kCT) k_impute_ckpt(CkptArgs a) {
   bool valid[kCJ];
 #pragma unroll
   for (int j = 0; j < kCJ; ++j) valid[j] = tid + kCT * j < K;
-  // warp-uniform: some thread of this warp holds state tid + 256 j (the other
-  // j are skipped by the whole warp; their values stay 0)
-  auto wlive = [&](int j) { return (tid & ~31) + kCT * j < K; };
   uint32_t w[kCJ];
   auto load_words = [&](int blk) {
 #pragma unroll
@@ -152,7 +149,6 @@ __global__ void __launch_bounds__(kCT) k_impute_ckpt(CkptArgs a) {
     float s[1] = {0.f};
 #pragma unroll
     for (int j = 0; j < kCJ; ++j) {
-      if (!wlive(j)) continue;
       const float pc = l == 0 ? f1 : fmaf(x[j], f2, f1);
       x[j] = valid[j] ? __fmul_rn(pc, (w[j] & m) ? ey : ex) : 0.f;
       s[0] = __fadd_rn(s[0], x[j]);
@@ -178,7 +174,7 @@ __global__ void __launch_bounds__(kCT) k_impute_ckpt(CkptArgs a) {
 #pragma unroll
     for (int j = 0; j < kCJ; ++j) {
       pc[j] = 0.f;
-      if (!wlive(j) || !valid[j]) continue;
+      if (!valid[j]) continue;
       const float p = last ? f1 : fmaf(xb[j], f2, f1);
       pc[j] = last ? 1.0f : p;
       xb[j] = __fmul_rn(p, (w[j] & m) ? ey : ex);
@@ -272,7 +268,6 @@ __global__ void __launch_bounds__(kCT) k_impute_ckpt(CkptArgs a) {
         float v[3] = {0.f, 0.f, 0.f};  // AlphaSum, prob_hid 0, prob_hid 1
 #pragma unroll
         for (int j = 0; j < kCJ; ++j) {
-          if (!wlive(j)) continue;
           const float p = l == 0 ? f1 : fmaf(x[j], f2, f1);
           const bool bit = (w[j] & m) != 0u;
           x[j] = valid[j] ? __fmul_rn(p, bit ? ey : ex) : 0.f;
@@ -323,7 +318,7 @@ __global__ void __launch_bounds__(kCT) k_impute_ckpt(CkptArgs a) {
         float v[3] = {0.f, 0.f, 0.f};  // betaSum, prob_hid 0, prob_hid 1
 #pragma unroll
         for (int j = 0; j < kCJ; ++j) {
-          if (!wlive(j) || !valid[j]) continue;
+          if (!valid[j]) continue;
           const bool bit = (w[j] & m) != 0u;
           const float al = scr[(size_t)(l - s0) * Kp + tid + kCT * j];
           const float p = fmaf(xb[j], f2, f1);
