@@ -26,7 +26,7 @@
 // are FP32 (with FP32 checkpoints they equal the first pass's bit for bit).
 // The log of every AlphaSum is accumulated in FP64: the chunk log-likelihood
 // sum_l log AlphaSum_l (the reference keeps no such value).
-// One CTA of 128 threads runs one chain; thread x owns states x + 128 j. The
+// One CTA of 256 threads runs one chain; thread x owns states x + 256 j. The
 // per-site sums are block reductions in one fixed tree.
 #include <cuda_bf16.h>
 
@@ -35,10 +35,7 @@
 namespace gp {
 namespace {
 
-// 128 threads (4 warps) per chain: at the batched workload the CTAs of all
-// chains are resident together and the SMs' issue is the bound, so fewer
-// threads per chain (less per-site reduction and control work) run more sites.
-constexpr int kCT = 128, kCW = kCT / 32;
+constexpr int kCT = 256, kCW = kCT / 32;
 
 struct CkptArgs {
   const int32_t* poly;
@@ -71,11 +68,11 @@ __device__ __forceinline__ void cta_sum(float (&v)[N], float (*red)[3][kCW], int
 #pragma unroll
     for (int i = 0; i < N; ++i) red[buf][i][threadIdx.x >> 5] = v[i];
   __syncthreads();
-  static_assert(kCW == 4, "four warps: one float4 of partials");
 #pragma unroll
   for (int i = 0; i < N; ++i) {
-    const float4 p = reinterpret_cast<const float4*>(red[buf][i])[0];
-    v[i] = __fadd_rn(__fadd_rn(p.x, p.y), __fadd_rn(p.z, p.w));
+    const float4 p = reinterpret_cast<const float4*>(red[buf][i])[0], q = reinterpret_cast<const float4*>(red[buf][i])[1];
+    v[i] = __fadd_rn(__fadd_rn(__fadd_rn(p.x, p.y), __fadd_rn(p.z, p.w)),
+                     __fadd_rn(__fadd_rn(q.x, q.y), __fadd_rn(q.z, q.w)));
   }
   buf ^= 1;
 }
@@ -89,7 +86,8 @@ __device__ __forceinline__ int ckpt_split(int np) { return (np / 2) & ~31; }
 template <int J, bool BF16, bool PB>
 __global__ void __launch_bounds__(kCT) k_impute_ckpt(CkptArgs a) {
   constexpr int kCJ = J;
-  __shared__ __align__(16) float red[2][3][kCW];  // rows of the warps' partials, read as one float4
+  static_assert(kCW == 8, "eight warps");
+  __shared__ __align__(16) float red[2][3][kCW];  // rows of 8 partials read as two float4
   int buf = 0;
   const int t = blockIdx.x >> 1, role = blockIdx.x & 1, tid = threadIdx.x;
   const int np = a.npoly[t], K = a.nstates[t];
@@ -375,12 +373,11 @@ int launch_impute_ckpt(ImputeWork& w, bool bf16, void* ckpt, float* csum, float*
     return GP_OK;                                                \
   }
   GP_CK_LAUNCH(2)
+  GP_CK_LAUNCH(3)
   GP_CK_LAUNCH(4)
+  GP_CK_LAUNCH(5)
   GP_CK_LAUNCH(6)
   GP_CK_LAUNCH(8)
-  GP_CK_LAUNCH(10)
-  GP_CK_LAUNCH(12)
-  GP_CK_LAUNCH(16)
 #undef GP_CK_LAUNCH
   return GP_OK;
 }
