@@ -527,13 +527,12 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   // heaviest targets start first and share an SM with the lightest.
   std::vector<int32_t> order(nb);
   std::vector<double> cost(nb);
-  int Kmax = 0, Kmin = 1 << 30;
+  int Kmax = 0;
   for (int b = 0; b < nb; ++b) {
     const int t = tsel_host.empty() ? b : tsel_host[b];
     order[b] = b;
     cost[b] = (double)cnt[b] * (1.0 + (double)((host_nstates[t] + kPhaseThreads - 1) / kPhaseThreads));
     Kmax = std::max(Kmax, host_nstates[t]);
-    Kmin = std::min(Kmin, host_nstates[t]);
   }
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
   // Placement 2, for batches of one to two entries per SM: the CTAs at grid
@@ -598,7 +597,7 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   std::vector<int64_t> offs(poff);
   offs.insert(offs.end(), ioff.begin(), ioff.end());
   cudaMemcpyAsync(p.offs.ptr, offs.data(), offs.size() * 8, cudaMemcpyHostToDevice, stream);
-  const int porder = fixed_porder ? fixed_porder : tune_porder;
+  const int porder = fixed_porder ? fixed_porder : 1;
   const bool paired_ok = !order_paired.empty() && chunk_start.size() == 2;
   cudaMemcpyAsync(p.order.ptr, (paired_ok && porder == 2 ? order_paired : order).data(), (size_t)nb * 4,
                   cudaMemcpyHostToDevice, stream);
@@ -621,44 +620,6 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
     pcells += 2.0 * 8.0 * (double)cnt[b] * (double)host_nstates[t];
   }
   launch_var_records(d_tsel, nb, w.poly.as<int32_t>(), L, panel.cm, mc, V, stream);
-  if (paired_ok && porder == 0 && Kmin != Kmax) {
-    // Autotune the placement on the first batch whose entries' state counts
-    // differ (where their work differs most): k_phase reads only its inputs and
-    // rewrites its own outputs, so it runs once per candidate with the same results.
-    if ((e = p.order2.ensure((size_t)nb * 4)) != cudaSuccess) return cuda_fail(e, "alloc order");
-    cudaMemcpyAsync(p.order2.ptr, order_paired.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, stream);
-    cudaEvent_t e0, e1, e2;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventCreate(&e2);
-    PhaseStore S2 = S;
-    S2.order = p.order2.as<int32_t>();
-    cudaEventRecord(e0, stream);
-    int lrc = launch_phase(J, d_tsel, nb, w.nstates.as<int32_t>(), w.hvar.as<uint32_t>(), w.WB, w.Kp,
-                           w.poly.as<int32_t>(), w.npoly.as<int32_t>(), L, panel.cm, V, S, mc, cfg.seed, iteration,
-                           d_target_ids, stream);
-    cudaEventRecord(e1, stream);
-    if (lrc == GP_OK)
-      lrc = launch_phase(J, d_tsel, nb, w.nstates.as<int32_t>(), w.hvar.as<uint32_t>(), w.WB, w.Kp,
-                         w.poly.as<int32_t>(), w.npoly.as<int32_t>(), L, panel.cm, V, S2, mc, cfg.seed, iteration,
-                         d_target_ids, stream);
-    cudaEventRecord(e2, stream);
-    const cudaError_t es = cudaEventSynchronize(e2);
-    float m1 = 0.f, m2 = 0.f;
-    cudaEventElapsedTime(&m1, e0, e1);
-    cudaEventElapsedTime(&m2, e1, e2);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaEventDestroy(e2);
-    if (lrc != GP_OK) return (fail(GP_E_ARG, "phasing: too many states"), GP_E_ARG);
-    if (es != cudaSuccess) return cuda_fail(es, "phasing placement tuning");
-    prof.kernel_launches += 2;
-    tune_ms[7] = m1;
-    tune_ms[8] = m2;
-    tune_porder = m2 < m1 ? 2 : 1;
-    if (tune_porder == 2)
-      cudaMemcpyAsync(p.order.ptr, p.order2.ptr, (size_t)nb * 4, cudaMemcpyDeviceToDevice, stream);
-  }
   cudaEvent_t ea;
   prof_begin(ea);
   for (size_t c = 0; c + 1 < chunk_start.size(); ++c) {
@@ -764,7 +725,6 @@ int gp_tuning_set(gp_ctx* ctx, int32_t chains_per_cta, int32_t sweep_haps_per_wa
   c.fixed_porder = phase_placement;
   if (!chains_per_cta) c.tune_cpc = 0;
   if (!sweep_haps_per_warp) c.tune_hpw = 0;
-  if (!phase_placement) c.tune_porder = 0;
   return GP_OK;
 }
 
@@ -774,7 +734,7 @@ int gp_tuning_get(gp_ctx* ctx, int32_t* chains_per_cta, int32_t* sweep_haps_per_
   Context& c = *reinterpret_cast<Context*>(ctx);
   if (chains_per_cta) *chains_per_cta = c.fixed_cpc ? c.fixed_cpc : c.tune_cpc;
   if (sweep_haps_per_warp) *sweep_haps_per_warp = c.fixed_hpw ? c.fixed_hpw : c.tune_hpw;
-  if (phase_placement) *phase_placement = c.fixed_porder ? c.fixed_porder : c.tune_porder;
+  if (phase_placement) *phase_placement = c.fixed_porder ? c.fixed_porder : 1;
   if (ms)
     for (int i = 0; i < 9; ++i) ms[i] = c.tune_ms[i];
   return GP_OK;

@@ -113,9 +113,9 @@ struct Context {
   // large enough to tell them apart; fixed_* (gp_tuning_set) override it.
   int tune_cpc = 0, tune_hpw = 0;     // chosen chains per CTA / haplotypes per sweep warp (0: not yet)
   int fixed_cpc = 0, fixed_hpw = 0;
-  // k_phase placement (1: entries in decreasing order of work; 2: the heaviest
-  // alone on an SM, the others paired heavy with light)
-  int tune_porder = 0, fixed_porder = 0;
+  // k_phase placement (1, the default: entries in decreasing order of work; 2:
+  // the heaviest alone on an SM, the others paired heavy with light)
+  int fixed_porder = 0;
   // phase-1 ms for 1, 2, 4 chains per CTA; sweep ms for 1, 2, 4, 8; k_phase ms for placements 1, 2
   float tune_ms[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   int sm_count = 0;

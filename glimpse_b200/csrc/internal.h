@@ -131,10 +131,10 @@ struct ImputeWork {
 struct PhaseWork {
   DevBuf rel, code, seg, miss, seg_start, counts, ytp, ytn, vflags, recb, recf;
   DevBuf pool;  // the stored segment-start and flat-het messages of one chunk of entries
-  DevBuf offs, pprob_sum, pprob_sumsum, iprob_sum, of1, dip, err, order, order2;
+  DevBuf offs, pprob_sum, pprob_sumsum, iprob_sum, of1, dip, err, order;
   std::vector<DevBuf*> all() {
     return {&rel, &code, &seg, &miss, &seg_start, &counts, &ytp, &ytn, &vflags, &recb, &recf, &pool, &offs,
-            &pprob_sum, &pprob_sumsum, &iprob_sum, &of1, &dip, &err, &order, &order2};
+            &pprob_sum, &pprob_sumsum, &iprob_sum, &of1, &dip, &err, &order};
   }
 };
 

@@ -348,11 +348,11 @@ int gp_learned_train(gp_ctx* ctx, int32_t kcand, float kpos, int32_t steps, int3
  * gp_tuning_get reports the shapes in use (0: not tuned yet) and, in ms[7],
  * the measured times (phase-1 chains for 1, 2, 4 chains per CTA, then the sweep
  * for 1, 2, 4, 8 haplotypes per warp; -1 where a shape did not fit, 0 where
- * not measured). A third choice is the placement of the phasing CTAs when a
- * batch has one to two entries per SM (phase_placement 1: entries in
+ * not measured). A third choice, set by the caller and not timed (the two
+ * measured alike), is the placement of the phasing CTAs when a batch has one
+ * to two entries per SM (phase_placement 1, the default: entries in
  * decreasing order of work; 2: the heaviest alone on an SM and the others
- * paired heaviest with lightest); ms must then hold 9 floats, the last two the
- * k_phase times of placements 1 and 2. */
+ * paired heaviest with lightest). ms holds 9 floats; the last two are 0. */
 int gp_tuning_set(gp_ctx* ctx, int32_t chains_per_cta, int32_t sweep_haps_per_warp, int32_t phase_placement);
 int gp_tuning_get(gp_ctx* ctx, int32_t* chains_per_cta, int32_t* sweep_haps_per_warp, int32_t* phase_placement,
                   float* ms);

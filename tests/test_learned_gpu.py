@@ -135,8 +135,7 @@ def test_autotuned_shapes_do_not_change_results():
 @pytest.mark.gpu
 def test_phasing_placement_does_not_change_results():
     """A batch of one to two targets per SM: the phasing placements (decreasing
-    work; heaviest alone, the rest paired) give identical haplotypes, and the
-    autotuner times both and reports its choice."""
+    work, the default; heaviest alone, the rest paired) give identical haplotypes."""
     import torch
     from glimpse_b200 import native, synth
     sms = torch.cuda.get_device_properties(0).multi_processor_count
@@ -156,8 +155,7 @@ def test_phasing_placement_does_not_change_results():
         h = [c.haps() for c in ctxs]
         for i in (1, 2):
             assert np.array_equal(h[0][0], h[i][0]) and np.array_equal(h[0][1], h[i][1])
-        _, _, placement, ms = ctxs[2].tuning()
-        assert placement in (1, 2) and ms[7] > 0 and ms[8] > 0
+        assert ctxs[2].tuning()[2] == 1 and ctxs[1].tuning()[2] == 2
     finally:
         for c in ctxs:
             c.close()
