@@ -324,14 +324,19 @@ __global__ void k_transpose_bf16(const __nv_bfloat16* __restrict__ in, int R, in
   }
 }
 
+// Columns of the per-block partial sums (hpart rows): dL/dw3 | dL/db2 | dL/db3,
+// loss | dL/db1. They are added over the blocks in block order (k_sum_head), so
+// a training step gives the same parameters on every run.
+constexpr int kHpW3 = 0, kHpB2 = kMlpHid, kHpB3 = 2 * kMlpHid, kHpLoss = 2 * kMlpHid + 1,
+              kHpB1 = 2 * kMlpHid + 2, kHpCols = 3 * kMlpHid + 2;
+
 // Loss head and the gradients it feeds, for rows [blockIdx.x * rpb, ...):
 // p = sigmoid(score), loss = wt * BCE(p, y) / n, ds = (p - y) * wt / n;
-// dz2[r][j] = ds * w3[j] where h2[r][j] > 0; accumulates dL/dw3, dL/db2,
-// dL/db3 and the loss. Thread j owns hidden unit j.
+// dz2[r][j] = ds * w3[j] where h2[r][j] > 0; the block's sums of dL/dw3, dL/db2,
+// dL/db3 and the loss go to its row of hpart. Thread j owns hidden unit j.
 __global__ void k_bwd_head(const float* __restrict__ score, const float* __restrict__ y, const float* __restrict__ wt,
                            const __nv_bfloat16* __restrict__ h2, const float* __restrict__ w3, int rows, int rpb,
-                           float inv_n, __nv_bfloat16* __restrict__ dz2, float* __restrict__ grad,
-                           float* __restrict__ loss) {
+                           float inv_n, __nv_bfloat16* __restrict__ dz2, float* __restrict__ hpart) {
   const int j = threadIdx.x;
   const int rb = blockIdx.x * rpb, re = min(rows, rb + rpb);
   const float w3j = w3[j];
@@ -350,21 +355,38 @@ __global__ void k_bwd_head(const float* __restrict__ score, const float* __restr
       ls += ww * inv_n * (fmaxf(s, 0.f) - s * yy + log1pf(expf(-fabsf(s))));
     }
   }
-  atomicAdd(&grad[kOffW3 + j], gw3);
-  atomicAdd(&grad[kOffB2 + j], gb2);
+  float* row = hpart + (size_t)blockIdx.x * kHpCols;
+  row[kHpW3 + j] = gw3;
+  row[kHpB2 + j] = gb2;
   if (j == 0) {
-    atomicAdd(&grad[kOffB3], gb3);
-    atomicAdd(loss, ls);
+    row[kHpB3] = gb3;
+    row[kHpLoss] = ls;
   }
 }
 
-// dst[j] += sum over rows of m[r][j] (m: [rows][256] BF16), thread j per column.
-__global__ void k_colsum(const __nv_bfloat16* __restrict__ m, int rows, int rpb, float* __restrict__ dst) {
+// The block's sums over rows of m[r][j] (m: [rows][256] BF16) into its row of
+// hpart (dL/db1 columns), thread j per column.
+__global__ void k_colsum(const __nv_bfloat16* __restrict__ m, int rows, int rpb, float* __restrict__ hpart) {
   const int j = threadIdx.x;
   const int rb = blockIdx.x * rpb, re = min(rows, rb + rpb);
   float acc = 0.f;
   for (int r = rb; r < re; ++r) acc += __bfloat162float(m[(size_t)r * kMlpHid + j]);
-  atomicAdd(&dst[j], acc);
+  hpart[(size_t)blockIdx.x * kHpCols + kHpB1 + j] = acc;
+}
+
+// The hpart columns added over the blocks in block order, into the gradient
+// vector and the loss.
+__global__ void k_sum_head(const float* __restrict__ hpart, int blocks, float* __restrict__ grad,
+                           float* __restrict__ loss) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < kHpCols; c += gridDim.x * blockDim.x) {
+    float v = 0.f;
+    for (int b = 0; b < blocks; ++b) v += hpart[(size_t)b * kHpCols + c];
+    if (c < kHpB2) grad[kOffW3 + c] = v;
+    else if (c < kHpB3) grad[kOffB2 + c - kHpB2] = v;
+    else if (c == kHpB3) grad[kOffB3] = v;
+    else if (c == kHpLoss) *loss = v;
+    else grad[kOffB1 + c - kHpB1] = v;
+  }
 }
 
 // dst[i] = sum over splits of part[z][i].
@@ -533,9 +555,10 @@ int mlp_train_device(Context& c, int n, int rows, float lr, bool want_grad) {
   const int rpb = 64;
   const int hb = (rows + rpb - 1) / rpb;
   float* g = M.grad.as<float>();
+  cudaError_t e;
+  if ((e = M.hpart.ensure((size_t)hb * kHpCols * 4)) != cudaSuccess) return c.cuda_fail(e, "mlp partial");
   k_bwd_head<<<hb, kMlpHid, 0, s>>>(M.score.as<float>(), M.y.as<float>(), M.wt.as<float>(), bf(M.h2),
-                                    params(M) + kOffW3, rows, rpb, 1.0f / (float)n, bf(M.dz2), g,
-                                    M.loss.as<float>());
+                                    params(M) + kOffW3, rows, rpb, 1.0f / (float)n, bf(M.dz2), M.hpart.as<float>());
   const dim3 tb(32, 8);
   k_transpose_bf16<<<dim3(rows / 32, kMlpHid / 32), tb, 0, s>>>(bf(M.dz2), rows, kMlpHid, bf(M.dz2t));
   k_transpose_bf16<<<dim3(rows / 32, kMlpHid / 32), tb, 0, s>>>(bf(M.h1), rows, kMlpHid, bf(M.h1t));
@@ -552,10 +575,11 @@ int mlp_train_device(Context& c, int n, int rows, float lr, bool want_grad) {
   ga.out_b = bf(M.dz1);
   ga.mask = bf(M.h1);
   ga.err = M.err.as<int>();
-  cudaError_t e = launch_gemm_tn(ga, 256, 1, 1, s);
+  e = launch_gemm_tn(ga, 256, 1, 1, s);
   if (e != cudaSuccess) return c.cuda_fail(e, "mlp dH1 launch");
   k_transpose_bf16<<<dim3(rows / 32, kMlpHid / 32), tb, 0, s>>>(bf(M.dz1), rows, kMlpHid, bf(M.dz1t));
-  k_colsum<<<hb, kMlpHid, 0, s>>>(bf(M.dz1), rows, rpb, g + kOffB1);
+  k_colsum<<<hb, kMlpHid, 0, s>>>(bf(M.dz1), rows, rpb, M.hpart.as<float>());
+  k_sum_head<<<(kHpCols + 255) / 256, 256, 0, s>>>(M.hpart.as<float>(), hb, g, M.loss.as<float>());
   // weight gradients, split over rows: dW2 = dz2^T h1, dW1 = dz1^T x
   const int kchunk = 2048;
   const int splits = (rows + kchunk - 1) / kchunk;
@@ -585,7 +609,7 @@ int mlp_train_device(Context& c, int n, int rows, float lr, bool want_grad) {
   g1.err = M.err.as<int>();
   if ((e = launch_gemm_tn(g1, 64, 0, splits, s)) != cudaSuccess) return c.cuda_fail(e, "mlp dW1 launch");
   k_sum_splits<<<64, 256, 0, s>>>(M.partial.as<float>(), kMlpHid * kMlpInP, splits, g + kOffW1);
-  c.prof.kernel_launches += 11;
+  c.prof.kernel_launches += 12;
   (void)want_grad;
   if (lr > 0.f) {
     M.step++;

@@ -27,13 +27,14 @@ struct MlpState {
   DevBuf m, v;                        // Adam moments over the packed parameter vector
   DevBuf grad;                        // packed FP32 gradient
   DevBuf partial;                     // split-K partial sums of the weight gradients
+  DevBuf hpart;                       // per-block partial sums of the small gradients and the loss
   int64_t step = 0;
   // per-batch scratch (rows padded to 128)
   DevBuf x, xt, y, wt, score, h1, h1t, h2, dz2, dz2t, dz1, dz1t, loss, err;
   DevBuf xf;                          // FP32 staging of host feature rows
   int cap_rows = 0;
   std::vector<DevBuf*> all() {
-    return {&param, &w1, &w2, &w2t, &m, &v, &grad, &partial, &x, &xt, &y, &wt, &score,
+    return {&param, &w1, &w2, &w2t, &m, &v, &grad, &partial, &hpart, &x, &xt, &y, &wt, &score,
             &h1, &h1t, &h2, &dz2, &dz2t, &dz1, &dz1t, &loss, &err, &xf};
   }
 };

@@ -184,3 +184,27 @@ def test_adaptive_set_size_stays_in_bounds():
         assert sizes[0.8].sum() <= sizes[0.2].sum()
     finally:
         ctx.close()
+
+
+@pytest.mark.gpu
+def test_training_is_deterministic():
+    """The training step's sums run in a fixed order (split-K partials and the
+    loss head's per-block partials added in block order, no float atomics), so
+    the same start gives the same parameters and losses on every run."""
+    from glimpse_b200 import native
+    w = _workload()
+    P, T = w.panel, w.targets
+    ctx = native.Context(P, kinit=300, kpbwt=120, pbwt_depth=8, pbwt_modulo_cm=0.05)
+    try:
+        ctx.set_targets(T, kpbwt=T.kpbwt)
+        ctx.iteration(native.STAGE_INIT, 0)
+        ctx.iteration(native.STAGE_BURN, 1)
+        runs = []
+        for _ in range(2):
+            ctx.mlp_init(5)
+            losses = ctx.learned_train(kcand=256, kpos=8.0, steps=20, batch=4096, lr=1e-3, seed=3)
+            runs.append((losses, ctx.mlp_params()))
+        assert np.array_equal(runs[0][0], runs[1][0])
+        assert np.array_equal(runs[0][1], runs[1][1])
+    finally:
+        ctx.close()
