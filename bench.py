@@ -364,6 +364,9 @@ def run_ours(args):
                                   (lambda tu: (*tu[:3], [round(float(x), 3) for x in tu[3]]))(ctx.tuning()))),
             "hmm_cells_per_s": world * hmm_cells / (ms / 1000.0),
             "dosage_r2": r2,
+            "dosage_r2_by_maf": [{"maf": [lo, hi], "sites": n_s, "r2": (None if r != r else round(r, 6))}
+                                 for lo, hi, n_s, r in synth.dosage_r2_bins(ds_h.numpy(), T.truth.sum(1),
+                                                                           synth.panel_maf(w.panel))],
             "gpu_launches": int(prof["kernel_launches"]),
             "clocks": clk,
             "roofline": roofline,

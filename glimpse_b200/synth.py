@@ -329,3 +329,35 @@ def dosage_r2(ds: np.ndarray, truth: np.ndarray) -> float:
         return 0.0
     r = ((x - x.mean()) * (y - y.mean())).mean() / (sx * sy)
     return float(r * r)
+
+
+# Allele-frequency bin edges of the r^2 report (GLIMPSE2_concordance --bins style).
+MAF_BINS = (0.0, 0.001, 0.002, 0.005, 0.01, 0.02, 0.05, 0.1, 0.2, 0.5)
+
+
+def dosage_r2_bins(ds: np.ndarray, truth: np.ndarray, maf: np.ndarray, edges=MAF_BINS):
+    """Dosage r^2 per minor-allele-frequency bin, as GLIMPSE2_concordance
+    reports it: a site goes to bin b when edges[b] < maf <= edges[b + 1]
+    (call_set::getFrequencyBin, concordance/src/containers/call_set_header.h:216-221),
+    and the bin's r^2 is the squared Pearson correlation of dosage and true
+    alt-allele count over all its (site, target) pairs
+    (call_set_reading.cpp:707, call_set_writing.cpp:245-249). ds, truth:
+    [targets][sites]; maf: [sites]. Returns (low, high, sites, r^2) per bin."""
+    ds = np.asarray(ds, np.float64)
+    truth = np.asarray(truth, np.float64)
+    maf = np.asarray(maf, np.float64)
+    out = []
+    for b in range(len(edges) - 1):
+        sel = (maf > edges[b]) & (maf <= edges[b + 1])
+        n = int(sel.sum())
+        r2 = dosage_r2(ds[:, sel], truth[:, sel]) if n else float("nan")
+        out.append((float(edges[b]), float(edges[b + 1]), n, r2))
+    return out
+
+
+def panel_maf(panel) -> np.ndarray:
+    """Minor-allele frequency of every panel site from its allele counts."""
+    cref = np.asarray(panel.cref, np.float64)
+    calt = np.asarray(panel.calt, np.float64)
+    return np.minimum(cref, calt) / np.maximum(cref + calt, 1.0)
+
