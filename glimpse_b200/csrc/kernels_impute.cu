@@ -130,21 +130,38 @@ __global__ void k_build_hvar(const int32_t* __restrict__ poly, const int32_t* __
   }
   const int w0 = r0 >> 5;
   const bool two = w0 + 1 < W;
-  int sh[32];  // bit of site i in the (word w0, word w0 + 1) pair, or -1 for a rare site
-#pragma unroll
-  for (int i = 0; i < 32; ++i) {
-    const int r = i < n ? s_row[i] : -1;
-    sh[i] = r >= 0 ? r - (w0 << 5) : -1;
+  // Runs of consecutive common sites of the block: their rows are consecutive
+  // too, so each run is one shifted bit field of the (word w0, word w0 + 1)
+  // pair (src: its first bit there, dst: its first site, len: its sites).
+  __shared__ uint32_t s_run[32];
+  __shared__ int s_nrun;
+  if (threadIdx.x == 0) {
+    int nr = 0;
+    for (int i = 0; i < n;) {
+      if (s_row[i] < 0) {
+        ++i;
+        continue;
+      }
+      int j = i;
+      while (j + 1 < n && s_row[j + 1] >= 0) ++j;
+      s_run[nr++] = (uint32_t)(s_row[i] - (w0 << 5)) | ((uint32_t)i << 8) | ((uint32_t)(j - i + 1) << 16);
+      i = j + 1;
+    }
+    s_nrun = nr;
   }
+  __syncthreads();
+  const int nrun = s_nrun;
   for (int k = threadIdx.x; k < Kp; k += blockDim.x) {
     uint32_t word = 0u;
     if (k < K) {
       const uint32_t* row = refT + (size_t)states[(size_t)t * Kp + k] * W + w0;
       const uint64_t pair = (uint64_t)row[0] | (two ? (uint64_t)row[1] << 32 : 0ull);
       word = rmaj;
-#pragma unroll
-      for (int i = 0; i < 32; ++i)
-        if (sh[i] >= 0) word |= (uint32_t)((pair >> sh[i]) & 1ull) << i;
+      for (int q = 0; q < nrun; ++q) {
+        const uint32_t rq = s_run[q];
+        const int src = rq & 0xff, dst = (rq >> 8) & 0xff, len = (int)(rq >> 16);
+        word |= (uint32_t)((pair >> src) & ((1ull << len) - 1ull)) << dst;
+      }
     }
     out[k] = word;
   }
