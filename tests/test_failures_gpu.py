@@ -60,3 +60,24 @@ def test_injected_allocation_failure_returns_nomem(small_workload, monkeypatch):
     finally:
         ctx.close()
         ref.close()
+
+
+@pytest.mark.gpu
+def test_invalid_configuration_and_tuning_are_refused(small_workload):
+    """A negative Kinit or Kpbwt is refused at context creation (the reference
+    exits there, caller_parameters.cpp:255-256), and tuning shapes outside their
+    candidates are refused without changing the context."""
+    from glimpse_b200 import native
+    w = small_workload
+    for kw in (dict(kinit=-1), dict(kpbwt=-5)):
+        with pytest.raises(native.GpError, match="status -1"):
+            native.Context(w.panel, pbwt_depth=8, pbwt_modulo_cm=0.05, **kw)
+    ctx = native.Context(w.panel, kinit=200, kpbwt=150, pbwt_depth=8, pbwt_modulo_cm=0.05)
+    try:
+        for args in ((3, 0, 0), (0, 3, 0), (0, 0, 3), (0, 0, -1)):
+            with pytest.raises(native.GpError, match="tuning"):
+                ctx.tuning_set(*args)
+        ctx.tuning_set(2, 1, 2)
+        assert ctx.tuning()[:3] == (2, 1, 2)
+    finally:
+        ctx.close()
