@@ -76,22 +76,22 @@ int Context::set_targets(int n, const uint8_t* gl, const uint8_t* flat, const in
 
 // Conditioning sets from states already on the device (impute.states with
 // stride Kp, impute.nstates): poly sites and Hvar. Copies K and npoly to the host.
+// The Hvar words are sized on the batch's largest polymorphic-site count (its
+// blocks of 32), not on all panel sites: the counts come back to the host
+// before the words are built.
 int Context::build_condsets_device(int n, int Kp) {
   ImputeWork& w = impute;
   const int L = panel.L;
   w.n = n;
   w.L = L;
   w.Kp = Kp;
-  w.WB = (L + 31) / 32;
   cudaError_t e;
   if ((e = w.mark.ensure((size_t)n * L)) != cudaSuccess) return cuda_fail(e, "alloc mark");
   if ((e = w.polyidx.ensure((size_t)n * L * 4)) != cudaSuccess) return cuda_fail(e, "alloc polyidx");
   if ((e = w.poly.ensure((size_t)n * L * 4)) != cudaSuccess) return cuda_fail(e, "alloc poly");
   if ((e = w.npoly.ensure(n * 4)) != cudaSuccess) return cuda_fail(e, "alloc npoly");
-  if ((e = w.hvar.ensure((size_t)n * w.WB * w.Kp * 4)) != cudaSuccess) return cuda_fail(e, "alloc hvar");
   launch_mark_poly(panel, w, stream);
   launch_compact_poly(panel, w, stream);
-  launch_build_hvar(panel, w, stream);
   impute_np.assign(n, 0);
   host_nstates.assign(n, 0);
   cudaMemcpyAsync(impute_np.data(), w.npoly.ptr, n * 4, cudaMemcpyDeviceToHost, stream);
@@ -101,6 +101,11 @@ int Context::build_condsets_device(int n, int Kp) {
     if (host_nstates[i] <= 0)
       return (fail(GP_E_DATA, "States for individual " + std::to_string(i) + " are zero. Error during selection."),
               GP_E_DATA);
+  int np_max = 1;
+  for (int i = 0; i < n; ++i) np_max = std::max(np_max, impute_np[i]);
+  w.WB = (np_max + 31) / 32;
+  if ((e = w.hvar.ensure((size_t)n * w.WB * w.Kp * 4)) != cudaSuccess) return cuda_fail(e, "alloc hvar");
+  launch_build_hvar(panel, w, stream);
   return GP_OK;
 }
 
