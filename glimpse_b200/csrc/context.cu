@@ -492,17 +492,20 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   PhaseWork& p = phase;
   const int L = panel.L;
   cudaError_t e;
-  if ((e = p.rel.ensure((size_t)nb * L * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
-  if ((e = p.code.ensure((size_t)nb * L)) != cudaSuccess) return cuda_fail(e, "alloc vars");
-  if ((e = p.seg.ensure((size_t)nb * L * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
-  if ((e = p.miss.ensure((size_t)nb * L * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
-  if ((e = p.seg_start.ensure((size_t)nb * (L + 2) * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  // per-entry VAR arrays and sums strided by the batch's largest poly count (VAR sites are poly sites)
+  int lv = 1;
+  for (int b = 0; b < nb; ++b) lv = std::max(lv, impute_np[tsel_host.empty() ? b : tsel_host[b]]);
+  if ((e = p.rel.ensure((size_t)nb * lv * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.code.ensure((size_t)nb * lv)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.seg.ensure((size_t)nb * lv * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.miss.ensure((size_t)nb * lv * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.seg_start.ensure((size_t)nb * (lv + 2) * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
   if ((e = p.counts.ensure((size_t)nb * 3 * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
-  if ((e = p.ytp.ensure((size_t)nb * L * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
-  if ((e = p.ytn.ensure((size_t)nb * L * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
-  if ((e = p.vflags.ensure((size_t)nb * L)) != cudaSuccess) return cuda_fail(e, "alloc vars");
-  if ((e = p.recb.ensure((size_t)nb * L * 16)) != cudaSuccess) return cuda_fail(e, "alloc vars");
-  if ((e = p.recf.ensure((size_t)nb * L * 16)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.ytp.ensure((size_t)nb * lv * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.ytn.ensure((size_t)nb * lv * 4)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.vflags.ensure((size_t)nb * lv)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.recb.ensure((size_t)nb * lv * 16)) != cudaSuccess) return cuda_fail(e, "alloc vars");
+  if ((e = p.recf.ensure((size_t)nb * lv * 16)) != cudaSuccess) return cuda_fail(e, "alloc vars");
   PhaseVars V;
   V.rel = p.rel.as<int32_t>();
   V.code = p.code.as<uint8_t>();
@@ -517,6 +520,7 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   V.nvar = p.counts.as<int32_t>();
   V.nseg = V.nvar + nb;
   V.nmiss = V.nvar + 2 * nb;
+  V.lv = lv;
   launch_build_vars(d_tsel, nb, w.poly.as<int32_t>(), w.npoly.as<int32_t>(), d_h0, d_h1, d_flat, panel.lq, L, V,
                     stream);
   prof.kernel_launches += 1;
@@ -558,11 +562,11 @@ int Context::run_phase(const int32_t* d_tsel, const std::vector<int32_t>& tsel_h
   // The per-entry buffers of fixed size come first, so that the budget below
   // sees the memory they leave.
   if ((e = p.offs.ensure((size_t)nb * 2 * 8)) != cudaSuccess) return cuda_fail(e, "alloc offs");
-  if ((e = p.pprob_sum.ensure((size_t)nb * (L + 2) * 8 * 4)) != cudaSuccess) return cuda_fail(e, "alloc psum");
-  if ((e = p.pprob_sumsum.ensure((size_t)nb * (L + 2) * 4)) != cudaSuccess) return cuda_fail(e, "alloc pss");
-  if ((e = p.iprob_sum.ensure((size_t)nb * L * 8 * 4)) != cudaSuccess) return cuda_fail(e, "alloc isum");
-  if ((e = p.of1.ensure((size_t)nb * L * 8 * 4)) != cudaSuccess) return cuda_fail(e, "alloc of1");
-  if ((e = p.dip.ensure((size_t)nb * (L + 2) * 4)) != cudaSuccess) return cuda_fail(e, "alloc dip");
+  if ((e = p.pprob_sum.ensure((size_t)nb * (lv + 2) * 8 * 4)) != cudaSuccess) return cuda_fail(e, "alloc psum");
+  if ((e = p.pprob_sumsum.ensure((size_t)nb * (lv + 2) * 4)) != cudaSuccess) return cuda_fail(e, "alloc pss");
+  if ((e = p.iprob_sum.ensure((size_t)nb * lv * 8 * 4)) != cudaSuccess) return cuda_fail(e, "alloc isum");
+  if ((e = p.of1.ensure((size_t)nb * lv * 8 * 4)) != cudaSuccess) return cuda_fail(e, "alloc of1");
+  if ((e = p.dip.ensure((size_t)nb * (lv + 2) * 4)) != cudaSuccess) return cuda_fail(e, "alloc dip");
   if ((e = p.err.ensure((size_t)nb * 4)) != cudaSuccess) return cuda_fail(e, "alloc err");
   if ((e = p.order.ensure((size_t)nb * 4)) != cudaSuccess) return cuda_fail(e, "alloc order");
   // The stored segment-start and flat-het messages of every entry, its two

@@ -38,11 +38,11 @@ __global__ void k_build_vars(const int32_t* __restrict__ poly, const int32_t* __
   const uint8_t* H0 = h0 + (size_t)t * L;
   const uint8_t* H1 = h1 + (size_t)t * L;
   const uint8_t* FL = flat + (size_t)t * L;
-  int32_t* vrel = V.rel + (size_t)b * L;
-  uint8_t* vcode = V.code + (size_t)b * L;
-  int32_t* vseg = V.seg + (size_t)b * L;
-  int32_t* vmiss = V.miss + (size_t)b * L;
-  int32_t* sstart = V.seg_start + (size_t)b * (L + 2);
+  int32_t* vrel = V.rel + (size_t)b * V.lv;
+  uint8_t* vcode = V.code + (size_t)b * V.lv;
+  int32_t* vseg = V.seg + (size_t)b * V.lv;
+  int32_t* vmiss = V.miss + (size_t)b * V.lv;
+  int32_t* sstart = V.seg_start + (size_t)b * (V.lv + 2);
   if (threadIdx.x < 3) carry[threadIdx.x] = 0;
   __syncthreads();
   for (int base = 0; base < np; base += THREADS * ITEMS) {
@@ -125,26 +125,26 @@ __global__ void k_var_records(const int32_t* __restrict__ tsel, const int32_t* _
   const int t = tsel ? tsel[b] : b;
   const int nv = V.nvar[b];
   const int32_t* pl = poly + (size_t)t * L;
-  const int32_t* vrel = V.rel + (size_t)b * L;
-  const int32_t* vseg = V.seg + (size_t)b * L;
-  const int32_t* sstart = V.seg_start + (size_t)b * (L + 2);
+  const int32_t* vrel = V.rel + (size_t)b * V.lv;
+  const int32_t* vseg = V.seg + (size_t)b * V.lv;
+  const int32_t* sstart = V.seg_start + (size_t)b * (V.lv + 2);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x) {
     const int s = pl[vrel[i]];
     float yn = 0.f;
     if (i + 1 < nv) yn = transition(cm, s, pl[vrel[i + 1]], mc);
-    V.yt_next[(size_t)b * L + i] = yn;
+    V.yt_next[(size_t)b * V.lv + i] = yn;
     float yp = 0.f;
     if (i > 0) yp = transition(cm, pl[vrel[i - 1]], s, mc);
-    V.yt_prev[(size_t)b * L + i] = yp;
+    V.yt_prev[(size_t)b * V.lv + i] = yp;
     const int seg = vseg[i];
     const int locus = i - sstart[seg];
     const int seglen = sstart[seg + 1] - sstart[seg];
     const int fl = (locus == 0 ? 1 : 0) | (locus == seglen - 1 ? 2 : 0);
-    V.flags[(size_t)b * L + i] = (uint8_t)fl;
-    const int x = vrel[i] | ((int)V.code[(size_t)b * L + i] << 24) | (fl << 28);
-    const int miss = V.miss[(size_t)b * L + i];
-    V.recb[(size_t)b * L + i] = make_int4(x, seg, miss, __float_as_int(yn));
-    V.recf[(size_t)b * L + i] = make_int4(x, seg, miss, __float_as_int(yp));
+    V.flags[(size_t)b * V.lv + i] = (uint8_t)fl;
+    const int x = vrel[i] | ((int)V.code[(size_t)b * V.lv + i] << 24) | (fl << 28);
+    const int miss = V.miss[(size_t)b * V.lv + i];
+    V.recb[(size_t)b * V.lv + i] = make_int4(x, seg, miss, __float_as_int(yn));
+    V.recf[(size_t)b * V.lv + i] = make_int4(x, seg, miss, __float_as_int(yp));
   }
 }
 
@@ -397,14 +397,14 @@ __global__ void __launch_bounds__(PT, 2) k_phase(const int32_t* __restrict__ tse
   fill_emission_table(sm.etab, mc, tid);  // read after the first barrier below
   const uint32_t* hv = hvar + (size_t)t * WB * Kp;
   const int nblk_poly = (npoly[t] + 31) >> 5;
-  const size_t vbase = (size_t)b * L;
+  const size_t vbase = (size_t)b * V.lv;
   float* PP = S.pprob + S.pprob_off[b];            // [nseg][K][8]
-  float* PPS = S.pprob_sum + (size_t)b * (L + 2) * 8;  // [nseg][8]
-  float* PPSS = S.pprob_sumsum + (size_t)b * (L + 2);  // [nseg]
+  float* PPS = S.pprob_sum + (size_t)b * (V.lv + 2) * 8;  // [nseg][8]
+  float* PPSS = S.pprob_sumsum + (size_t)b * (V.lv + 2);  // [nseg]
   float* IP = S.iprob + S.iprob_off[b];            // [nmiss][K][8]
-  float* IPS = S.iprob_sum + (size_t)b * L * 8;     // [nmiss][8]
-  float* OF1 = S.of1 + (size_t)b * L * 8;           // [nmiss][8]
-  int32_t* dip = S.dip + (size_t)b * (L + 2);
+  float* IPS = S.iprob_sum + (size_t)b * V.lv * 8;  // [nmiss][8]
+  float* OF1 = S.of1 + (size_t)b * V.lv * 8;        // [nmiss][8]
+  int32_t* dip = S.dip + (size_t)b * (V.lv + 2);
   const uint32_t rng_target = target_ids ? (uint32_t)target_ids[b] : (uint32_t)t;
   const int nvb = (nv + 31) >> 5;
 
@@ -639,20 +639,20 @@ __global__ void k_phase_writeback(const int32_t* __restrict__ tsel, const int32_
   const int nseg = V.nseg[b];
   const uint32_t rng_target = target_ids ? (uint32_t)target_ids[b] : (uint32_t)t;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x) {
-    const int code = V.code[(size_t)b * L + i];
+    const int code = V.code[(size_t)b * V.lv + i];
     const int typ = code & 7;
     if (typ == VT_HOM) continue;
-    const int l = V.rel[(size_t)b * L + i];
+    const int l = V.rel[(size_t)b * V.lv + i];
     const int s = poly[(size_t)t * L + l];
-    const int seg = V.seg[(size_t)b * L + i];
-    const int i0 = S.dip[(size_t)b * (L + 2) + seg];
+    const int seg = V.seg[(size_t)b * V.lv + i];
+    const int i0 = S.dip[(size_t)b * (V.lv + 2) + seg];
     const int i1 = 7 - i0;
     if (typ < 3) {
       h0[(size_t)t * L + s] = (uint8_t)hyp_allele(i0, typ);
       h1[(size_t)t * L + s] = (uint8_t)hyp_allele(i1, typ);
     } else {
-      const int m = V.miss[(size_t)b * L + i];
-      const float* of = S.of1 + ((size_t)b * L + m) * 8;
+      const int m = V.miss[(size_t)b * V.lv + i];
+      const float* of = S.of1 + ((size_t)b * V.lv + m) * 8;
       const float h0a0 = 1.0f - of[i0], h0a1 = of[i0];
       const float h1a0 = 1.0f - of[i1], h1a1 = of[i1];
       float p01 = __fmul_rn(fmaf(h0a0, mc.ee_phs, __fmul_rn(h0a1, mc.ed_phs)),

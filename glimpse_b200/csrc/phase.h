@@ -28,6 +28,9 @@ struct PhaseVars {
   int32_t* nvar;
   int32_t* nseg;
   int32_t* nmiss;
+  // Per-entry stride of the arrays above and of PhaseStore's per-entry sums:
+  // the batch's largest polymorphic-site count (VAR sites are a subset).
+  int lv;
 };
 
 struct PhaseStore {
