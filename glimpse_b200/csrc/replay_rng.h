@@ -4,7 +4,7 @@
 // (common/src/utils/random_number.h:35-60, global `rng` in
 // common/src/utils/otools.h:122), in an order that depends on the data and,
 // with --threads > 1, on thread scheduling. A batched GPU path cannot follow
-// one sequential engine, so this build keys an independent stream on
+// one sequential engine, so the library keys an independent stream on
 // (seed, purpose, iteration, target) and generates it with Philox4x32-10
 // (Salmon, Moraes, Dror, Shaw: "Parallel random numbers: as easy as 1, 2, 3",
 // SC'11). Word i of a stream is lane (i & 3) of Philox(counter = {i >> 2,

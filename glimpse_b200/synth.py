@@ -1,6 +1,6 @@
 """Seeded synthetic panels, targets and genotype likelihoods.
 
-No public dataset ships with this build, so the GLIMPSE2_phase workloads are
+No public dataset ships with the project, so the GLIMPSE2_phase workloads are
 generated: a reference panel of haplotypes copied as a Li-Stephens mosaic of a
 few founders (with copying errors) at common sites, sparse rare alleles placed
 on haplotypes that share a founder segment, held-out mosaic haplotypes paired
