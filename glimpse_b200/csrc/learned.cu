@@ -652,9 +652,10 @@ int Context::learned_select_states(int stage, int iteration, int& Kp) {
   // Feature rows and their scores in chunks of targets whose rows fit the
   // memory budget (the rows are 128 B each; the scores are kept for all).
   const size_t row_bytes = (size_t)kMlpInP * 2;
-  // at most 2 GiB of rows at a time (16M rows, hundreds of waves of the
-  // network's 128-row tiles), so that the rows do not take the stores' memory
-  const size_t budget = std::min<size_t>(store_budget(lw.x.cap, rows * row_bytes), size_t(2) << 30);
+  // at most 8 GiB of rows at a time (64M rows), so that the rows do not take
+  // the stores' memory; the device is asked only when the buffer must grow
+  const size_t want = std::min<size_t>(rows * row_bytes, size_t(8) << 30);
+  const size_t budget = store_budget(lw.x.cap, want);
   const int nc = (int)std::max<size_t>(1, std::min<size_t>(n, budget / (per_t * row_bytes)));
   if ((e = lw.x.ensure((size_t)nc * per_t * row_bytes)) != cudaSuccess) return cuda_fail(e, "learned features alloc");
   for (int t0 = 0; t0 < n; t0 += nc) {
