@@ -99,6 +99,37 @@ def test_disabling_restores_plain_selection():
 
 
 @pytest.mark.gpu
+def test_feature_chunks_do_not_change_selection(monkeypatch):
+    """The learned selection computes feature rows and their scores in chunks of
+    targets when the rows do not fit the memory budget together
+    (GLIMPSE_B200_STORE_BUDGET_MB lowers the budget so that each chunk holds one
+    or two of these targets). The conditioning sets and haplotypes must be
+    identical to the run whose rows fit at once."""
+    from glimpse_b200 import native
+    w = _workload()
+    P, T = w.panel, w.targets
+    kw = dict(kinit=300, kpbwt=120, pbwt_depth=8, pbwt_modulo_cm=0.05)
+    a, b = native.Context(P, **kw), native.Context(P, **kw)
+    try:
+        for c in (a, b):
+            c.set_targets(T, kpbwt=T.kpbwt)
+            c.iteration(native.STAGE_INIT, 0)
+            c.mlp_init(5)
+            c.learned_enable(True, kcand=400)
+        a.iteration(native.STAGE_BURN, 1)
+        monkeypatch.setenv("GLIMPSE_B200_STORE_BUDGET_MB", "1")
+        b.iteration(native.STAGE_BURN, 1)
+        monkeypatch.delenv("GLIMPSE_B200_STORE_BUDGET_MB")
+        for t in range(T.n):
+            assert np.array_equal(a.states(t), b.states(t))
+        ha, hb = a.haps(), b.haps()
+        assert np.array_equal(ha[0], hb[0]) and np.array_equal(ha[1], hb[1])
+    finally:
+        a.close()
+        b.close()
+
+
+@pytest.mark.gpu
 def test_autotuned_shapes_do_not_change_results():
     """The autotuner picks chains per CTA (imputation) and haplotypes per warp
     (PBWT sweep) by timing; results must not depend on either. Two contexts
