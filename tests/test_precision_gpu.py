@@ -99,6 +99,27 @@ def test_checkpointed_fp32_posteriors_and_loglik():
         assert abs(ll[i] - llr) <= 1e-6 * n_poly, (i, ll[i], llr)
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("K", [700, 1000, 1500, 2000])
+def test_checkpointed_states_per_thread_instances(K):
+    """Each launch instantiates the checkpointed kernel for the smallest J (states
+    per thread, 256 threads) that holds its largest K: K = 700, 1000, 1500 and 2000
+    reach J = 3, 4, 6 and 8, the instances the other tests (J = 2 and 5) do not.
+    FP32 checkpoints: HP within 1e-5 of the FP64 restatement and of the full
+    store, the chunk log-likelihood within 1e-6 per site."""
+    from glimpse_b200 import native, synth
+    w = synth.make_panel_and_targets(2048, 6000, 0.5, 0.5, 2, ("uniform", 0.5, 2.0), ("fixed", 200), seed=53,
+                                     sparse_maf=0.005)
+    out, ref = _impute_modes(w, [K, K // 3], 6, [native.PRECISION_FULL, native.PRECISION_CKPT_F32])
+    hp_full, _ = out[native.PRECISION_FULL]
+    hp_ck, ll = out[native.PRECISION_CKPT_F32]
+    for i, (hr, llr) in enumerate(ref):
+        e = float(np.abs(hp_ck[i].astype(np.float64) - hr.astype(np.float64)).max())
+        assert e <= TOL, f"K={K} haplotype {i}: max |HP - HP_fp64| = {e:.3e}"
+        assert float(np.abs(hp_ck[i] - hp_full[i]).max()) <= TOL
+        assert abs(ll[i] - llr) <= 1e-6 * w.panel.n_sites, (i, ll[i], llr)
+
+
 def _dosage(hp0, hp1):
     return hp0[1::2].astype(np.float64) + hp1[1::2].astype(np.float64)
 
