@@ -46,6 +46,37 @@ def test_rephase_matches_reference(small_workload):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("K", [200, 900, 1400, 1700, 2000])
+def test_rephase_states_per_thread_instances(K):
+    """k_phase is instantiated for the smallest J (states per thread, 256 threads)
+    that holds the launch's largest K. One K per call reaches J = 1, 4, 6, 7 and 8
+    (the test above runs J = 3; the iteration tests J = 2 and 5); the sampled
+    haplotypes must equal rephaseHaplotypes' on identical inputs and streams."""
+    O = ref_oracle_or_skip()
+    from glimpse_b200 import native, synth
+    w = synth.make_panel_and_targets(2048, 6000, 0.5, 0.5, 2, ("uniform", 0.5, 2.0), ("fixed", 200), seed=59,
+                                     sparse_maf=0.005)
+    P, T = w.panel, w.targets
+    orc = O.RefOracle(P, T, kinit=200, kpbwt=150)
+    ctx = native.Context(P)
+    try:
+        rng = np.random.default_rng(K)
+        cases = []
+        for t in range(T.n):
+            s = np.sort(rng.choice(P.n_ref_haps, size=K, replace=False)).astype(np.uint32)
+            cases.append((s, _noisy_haps(rng, T.truth[t, 0]), _noisy_haps(rng, T.truth[t, 1]), T.flat[t], t))
+        it = 2
+        refs = [orc.rephase(s, h0, h1, fl, it, tid) for (s, h0, h1, fl, tid) in cases]
+        g0, g1 = ctx.rephase_batch([c[0] for c in cases], np.stack([c[1] for c in cases]),
+                                   np.stack([c[2] for c in cases]), np.stack([c[3] for c in cases]), it,
+                                   target_ids=[c[4] for c in cases])
+        for i, (r0, r1, _) in enumerate(refs):
+            assert np.array_equal(g0[i], r0) and np.array_equal(g1[i], r1), (K, i)
+    finally:
+        ctx.close()
+
+
+@pytest.mark.gpu
 def test_invalid_diplotype_sums_return_data_error(small_workload):
     """SAMPLE_DIP with a NaN, infinite or sub-normal sum: the reference stops on
     an assertion (phasing_hmm.cpp:175); the library finishes the call and

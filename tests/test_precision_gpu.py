@@ -106,7 +106,9 @@ def test_checkpointed_states_per_thread_instances(K):
     per thread, 256 threads) that holds its largest K: K = 700, 1000, 1500 and 2000
     reach J = 3, 4, 6 and 8, the instances the other tests (J = 2 and 5) do not.
     FP32 checkpoints: HP within 1e-5 of the FP64 restatement and of the full
-    store, the chunk log-likelihood within 1e-6 per site."""
+    store, the chunk log-likelihood within 1e-6 per site. The full store's own
+    kernel (one warp per chain, J = K / 128 quads rounded up) runs at J = 6, 8, 12
+    and 16 here, and its HP must be within 1e-5 of FP64 as well."""
     from glimpse_b200 import native, synth
     w = synth.make_panel_and_targets(2048, 6000, 0.5, 0.5, 2, ("uniform", 0.5, 2.0), ("fixed", 200), seed=53,
                                      sparse_maf=0.005)
@@ -116,6 +118,8 @@ def test_checkpointed_states_per_thread_instances(K):
     for i, (hr, llr) in enumerate(ref):
         e = float(np.abs(hp_ck[i].astype(np.float64) - hr.astype(np.float64)).max())
         assert e <= TOL, f"K={K} haplotype {i}: max |HP - HP_fp64| = {e:.3e}"
+        ef = float(np.abs(hp_full[i].astype(np.float64) - hr.astype(np.float64)).max())
+        assert ef <= TOL, f"K={K} haplotype {i}, full store: max |HP - HP_fp64| = {ef:.3e}"
         assert float(np.abs(hp_ck[i] - hp_full[i]).max()) <= TOL
         assert abs(ll[i] - llr) <= 1e-6 * w.panel.n_sites, (i, ll[i], llr)
 
