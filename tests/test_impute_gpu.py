@@ -36,6 +36,36 @@ def test_impute_matches_reference(small_workload):
 
 
 @pytest.mark.gpu
+def test_impute_every_quad_count_matches_reference():
+    """k_impute_warp is instantiated for J = 1..16 quads per lane (one warp per
+    chain, J = the launch's largest K / 128 rounded up). One call per J, with
+    K = 128 J - 17 for the first haplotype and half of it for the second; HP
+    within 1e-5 of computePosteriors on each."""
+    O = ref_oracle_or_skip()
+    from glimpse_b200 import native, synth
+    w = synth.make_panel_and_targets(2048, 6000, 0.5, 0.5, 2, ("uniform", 0.5, 2.0), ("fixed", 200), seed=61,
+                                     sparse_maf=0.005)
+    P, T = w.panel, w.targets
+    orc = O.RefOracle(P, T, kinit=200, kpbwt=150)
+    ctx = native.Context(P)
+    rng = np.random.default_rng(13)
+    try:
+        for J in range(1, 17):
+            states, hls, flats, refs = [], [], [], []
+            for t, K in enumerate((128 * J - 17, (128 * J - 17) // 2)):
+                s = _random_states(rng, P.n_ref_haps, K)
+                hl = init_hl(T.gl[t], T.flat[t])
+                refs.append(orc.impute(s, hl, T.flat[t])[0])
+                states.append(s); hls.append(hl); flats.append(T.flat[t])
+            hp = ctx.impute_batch(states, np.stack(hls), np.stack(flats))
+            for i, r in enumerate(refs):
+                err = float(np.abs(hp[i] - r).max())
+                assert err <= TOL, f"J={J} haplotype {i}: max |dHP| = {err:.3e}"
+    finally:
+        ctx.close()
+
+
+@pytest.mark.gpu
 def test_chunked_store_matches_single_launch(small_workload, monkeypatch):
     """When the haplotypes' forward-backward stores do not fit the device-memory
     budget together, they run in consecutive chunks (GLIMPSE_B200_STORE_BUDGET_MB
