@@ -177,15 +177,17 @@ class ReferenceRun:
     unmodified) on the host cores: one step is one complete run, 1 init +
     burn-in + main iterations and finalisation, over a fixed subset of the
     workload's targets, with the reference driver's dynamic assignment of
-    targets to threads and per-thread replay streams."""
+    targets to threads and per-thread replay streams; or, with native_rng, the
+    reference's own generator (std::mt19937 seeded once) on one thread."""
 
-    def __init__(self, w, n_targets, threads):
+    def __init__(self, w, n_targets, threads, native_rng=False):
         from oracle import oracle as O
         self.O = O
         self.w = w
         self.sub = subset(w.targets, n_targets)
-        self.threads = threads
-        self.orc = O.RefOracle(w.panel)
+        self.native_rng = native_rng
+        self.threads = 1 if native_rng else threads
+        self.orc = O.RefOracle(w.panel, native_rng=native_rng)
 
     def step(self):
         O, sub = self.O, self.sub
@@ -202,7 +204,9 @@ class ReferenceRun:
     def sample_text(self, seconds):
         return (f"{self.sub.n} of the {self.w.targets.n} targets (the first {self.sub.n}), one complete run per "
                 f"step (1 init + {BURNIN} burn-in + {MAIN} main iterations and finalisation, {seconds:.1f} s) on "
-                f"{self.threads} threads (per-thread replay RNG); samples/s = targets / run time")
+                f"{self.threads} threads ("
+                + ("the reference's own std::mt19937" if self.native_rng else "per-thread replay RNG")
+                + "); samples/s = targets / run time")
 
 
 def default_subset(threads):
@@ -215,15 +219,17 @@ def run_reference(args):
         return 0
     try:
         from oracle import oracle as O
-        if not O.ref_available():
-            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libglimpse_ref.so not built"}))
+        native = getattr(args, "ref_rng", "replay") == "native"
+        if not O.ref_available(native_rng=native):
+            lib = "libglimpse_ref_native.so" if native else "libglimpse_ref.so"
+            print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref/{lib} not built"}))
             return 0
     except Exception as e:  # pragma: no cover
         print(json.dumps({"impl": "reference", "unavailable": f"oracle import failed: {e}"}))
         return 0
     w = synth.workload(args.config, seed=1)
-    threads = os.cpu_count() or 1
-    ref = ReferenceRun(w, args.subset or default_subset(threads), threads)
+    threads = 1 if native else (os.cpu_count() or 1)
+    ref = ReferenceRun(w, args.subset or default_subset(threads), threads, native_rng=native)
     for _ in range(args.warmup):
         ref.step()
     times = [ref.step() for _ in range(args.steps)]
@@ -233,7 +239,7 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_run * 1000.0, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": workload_label(args.config), "parallelism": f"{threads} host threads",
-                       "targets_timed": ref.sub.n},
+                       "targets_timed": ref.sub.n, "rng": "native" if native else "replay"},
             "dosage_r2": ref.dosage_r2(),
             "cpu_baseline": {"value": value, "unit": "samples/s", "cores": threads, "kind": "reference",
                              "sample": ref.sample_text(t_run)},
@@ -634,6 +640,9 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--ref-rng", choices=["replay", "native"], default="replay",
+                    help="reference arm: replay streams on every host thread (default), or the reference's own "
+                         "std::mt19937 on one thread")
     ap.add_argument("--config", default="batched")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--subset", type=int, default=0,

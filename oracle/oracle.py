@@ -2,7 +2,10 @@
 
 ctypes bindings for
   * oracle/_ref/libglimpse_ref.so: the reference's own hot-path sources compiled
-    unmodified (oracle/Makefile) behind a C-ABI harness (oracle/ref_harness.cpp);
+    unmodified (oracle/Makefile) behind a C-ABI harness (oracle/ref_harness.cpp),
+    drawing from the replay streams the GPU path also uses;
+  * oracle/_ref/libglimpse_ref_native.so: the same with the reference's own
+    random-number generator (std::mt19937 seeded once, one thread);
   * oracle/_ref/librestate.so: the FP64/FP32 restatement (oracle/restate.c).
 
 Only tests/, __graft_entry__.smoke() and bench.py's reference arm load this
@@ -17,11 +20,12 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.environ.get("GP_ORACLE_LIB", os.path.join(HERE, "_ref", "libglimpse_ref.so"))
+REF_LIB_NATIVE = os.path.join(HERE, "_ref", "libglimpse_ref_native.so")
 RESTATE_LIB = os.path.join(HERE, "_ref", "librestate.so")
 
 STAGE_INIT, STAGE_BURN, STAGE_MAIN = 0, 1, 2
 
-_ref = None
+_ref = {}
 _restate = None
 
 
@@ -29,14 +33,14 @@ def _p(a, ctype):
     return a.ctypes.data_as(C.POINTER(ctype)) if a is not None else None
 
 
-def ref_available() -> bool:
-    return os.path.exists(REF_LIB)
+def ref_available(native_rng=False) -> bool:
+    return os.path.exists(REF_LIB_NATIVE if native_rng else REF_LIB)
 
 
-def ref_lib():
-    global _ref
-    if _ref is None:
-        lib = C.CDLL(REF_LIB)
+def ref_lib(native_rng=False):
+    """The harness library: replay streams (default) or the reference's own generator."""
+    if native_rng not in _ref:
+        lib = C.CDLL(REF_LIB_NATIVE if native_rng else REF_LIB)
         vp = C.c_void_p
         lib.orc_create.restype = vp
         lib.orc_create.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
@@ -80,22 +84,35 @@ def ref_lib():
         lib.orc_unphred.argtypes = [C.POINTER(C.c_float)]
         lib.orc_stream_words.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_int,
                                          C.POINTER(C.c_uint32)]
-        lib.orc_rng_floats.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.POINTER(C.c_float)]
-        lib.orc_rng_ints.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.POINTER(C.c_uint32),
-                                     C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]
-        lib.orc_std_sample.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int,
-                                       C.POINTER(C.c_int32), C.POINTER(C.c_uint64)]
+        if not native_rng:  # the shimmed class's stream draws exist in the replay build only
+            lib.orc_rng_floats.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
+                                           C.POINTER(C.c_float)]
+            lib.orc_rng_ints.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
+                                         C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                         C.POINTER(C.c_uint64)]
+            lib.orc_std_sample.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int,
+                                           C.POINTER(C.c_int32), C.POINTER(C.c_uint64)]
         lib.orc_philox.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
-        _ref = lib
-    return _ref
+        lib.orc_native_rng.restype = C.c_int
+        if lib.orc_native_rng() != int(bool(native_rng)):
+            raise RuntimeError("oracle library built with the other random-number generator")
+        _ref[native_rng] = lib
+    return _ref[native_rng]
 
 
 class RefOracle:
-    """The reference's GLIMPSE2_phase hot path on the host (one object per panel)."""
+    """The reference's GLIMPSE2_phase hot path on the host (one object per panel).
+
+    native_rng=True runs it with the reference's own generator (std::mt19937
+    seeded once, caller_initialise.cpp:49; draws in the reference's call order,
+    so on one thread only) in place of the replay streams; call-level parity
+    with the GPU then no longer holds, only run-level statistics such as r2."""
 
     def __init__(self, panel, targets=None, *, ne=100000, err_imp=1e-12, err_phase=1e-4, min_gl=1e-10,
-                 pbwt_depth=12, pbwt_modulo_cm=0.1, kinit=1000, kpbwt=2000, kpbwt_target=None, seed=15052011):
-        lib = ref_lib()
+                 pbwt_depth=12, pbwt_modulo_cm=0.1, kinit=1000, kpbwt=2000, kpbwt_target=None, seed=15052011,
+                 native_rng=False):
+        lib = ref_lib(native_rng)
+        self.native_rng = bool(native_rng)
         self.lib = lib
         self.panel = panel
         p = panel

@@ -18,6 +18,7 @@
 // access-specifier override below only reaches the two model classes (their
 // private message buffers are read back for parity checks).
 #include <utils/otools.h>
+#include "../glimpse_b200/csrc/replay_rng.h"
 #include <containers/bitmatrix.h>
 #include <containers/variant_map.h>
 #include <containers/haplotype_set.h>
@@ -40,6 +41,23 @@ string_utils stb;
 timer tac;
 
 namespace {
+
+// Stream control. The replay engine is pointed at the (purpose, iteration,
+// target) stream before each call that draws. The native-RNG build (the
+// reference's own std::mt19937, GP_NATIVE_RNG) is seeded once, as
+// caller_initialise.cpp:49 does, and draws in the reference's call order, so
+// both are no-ops there.
+#ifdef GP_NATIVE_RNG
+constexpr bool kNativeRng = true;
+inline void rng_select(uint32_t, uint32_t, uint32_t) {}
+inline void rng_reseed(uint64_t) {}
+#else
+constexpr bool kNativeRng = false;
+inline void rng_select(uint32_t purpose, uint32_t iteration, uint32_t target) {
+  rng.randomEngine.select(purpose, iteration, target);
+}
+inline void rng_reseed(uint64_t seed) { rng.randomEngine.seed_with(seed); }
+#endif
 
 struct Worker {
   std::unique_ptr<conditioning_set> cond;
@@ -94,14 +112,14 @@ void phase_individual(Oracle& o, Worker& w, int ind, int stage, int iter_index) 
     else g->initHaplotypeLikelihoods(w.HLC, o.min_gl);
   }
   w.hmm->computePosteriors(w.HLC, g->flat, w.HP0);
-  rng.randomEngine.select(gp::RNG_SAMPLE_H0, iter_index, ind);
+  rng_select(gp::RNG_SAMPLE_H0, iter_index, ind);
   g->sampleHaplotypeH0(w.HP0);
   if (ploidy > 1) {
     g->makeHaplotypeLikelihoods(w.HLC, false, o.min_gl);
     w.hmm->computePosteriors(w.HLC, g->flat, w.HP1);
-    rng.randomEngine.select(gp::RNG_SAMPLE_H1, iter_index, ind);
+    rng_select(gp::RNG_SAMPLE_H1, iter_index, ind);
     g->sampleHaplotypeH1(w.HP1);
-    rng.randomEngine.select(gp::RNG_PHASE, iter_index, ind);
+    rng_select(gp::RNG_PHASE, iter_index, ind);
     w.dmm->rephaseHaplotypes(g->H0, g->H1, g->flat);
   }
   if (stage == STAGE_MAIN) {
@@ -116,9 +134,15 @@ void phase_individual(Oracle& o, Worker& w, int ind, int stage, int iter_index) 
 
 // Init-stage selection (haplotype_set.cpp:775-833) run one target at a time so
 // that each target draws from its own stream (target index moved to slot 0).
+// The native-RNG build runs it over all targets in one call, as
+// caller_algorithm.cpp:91 does.
 void init_selection(Oracle& o, int iter_index) {
   haplotype_set& H = o.H;
   if (H.Kinit == 0) return;
+  if (kNativeRng) {
+    H.performSelection_RARE_INIT_GL(o.V);
+    return;
+  }
   std::vector<std::vector<int>> sind = H.SindTarGL;
   const unsigned int n_tar = H.n_tar_samples;
   std::vector<std::set<int>> result(n_tar);
@@ -128,7 +152,7 @@ void init_selection(Oracle& o, int iter_index) {
     H.SindTarGL.assign(1, sind[i]);
     H.init_states.assign(1, std::set<int>());
     H.tar_ind2hapid.assign(1, ind2hap[i]);
-    rng.randomEngine.select(gp::RNG_INIT_SEL, iter_index, i);
+    rng_select(gp::RNG_INIT_SEL, iter_index, i);
     H.performSelection_RARE_INIT_GL(o.V);
     result[i] = H.init_states[0];
   }
@@ -140,13 +164,15 @@ void init_selection(Oracle& o, int iter_index) {
 
 // caller::phase_iteration (caller_algorithm.cpp:86-126) without checkpoint.
 void phase_iteration(Oracle& o, int stage, int iter_index, int n_threads) {
+  if (kNativeRng && n_threads > 1)
+    throw std::runtime_error("the reference's own generator is one global stream: run it on one thread");
   if (stage == STAGE_INIT) {
     o.H.initRareTar(o.G, o.V);
     init_selection(o, iter_index);
   } else {
     o.H.updateHaplotypes(o.G);
     o.H.transposeRareTar();
-    rng.randomEngine.select(gp::RNG_PBWT, iter_index, 0);
+    rng_select(gp::RNG_PBWT, iter_index, 0);
     o.H.matchHapsFromCompressedPBWTSmall(o.V, stage == STAGE_MAIN);
   }
   const int n_ind = o.G.n_ind;
@@ -161,7 +187,7 @@ void phase_iteration(Oracle& o, int stage, int iter_index, int n_threads) {
     for (int t = 0; t < n_threads; ++t) {
       pool.emplace_back([&]() {
         rng.setSeed((unsigned int)o.seed);
-        rng.randomEngine.seed_with(o.seed);
+        rng_reseed(o.seed);
         auto w = make_worker(o, o.kpbwt);
         for (;;) {
           const int i = next.fetch_add(1);
@@ -337,7 +363,7 @@ int orc_config(void* p, int ne, float err_imp, float err_phase, float min_gl, in
     if (kpbwt_target)
       for (int i = 0; i < o->G.n_ind; ++i) o->kpbwt_target[i] = kpbwt_target[i];
     rng.setSeed((unsigned int)seed);
-    rng.randomEngine.seed_with(seed);
+    rng_reseed(seed);
     const int kp = std::min(kpbwt, (int)o->H.n_ref_haps);
     const int ki = std::min(kinit, (int)o->H.n_ref_haps);
     o->H.allocatePBWT(pbwt_depth, pbwt_modulo_cm, o->V, o->G, ki, kp);
@@ -349,7 +375,7 @@ int orc_config(void* p, int ne, float err_imp, float err_phase, float min_gl, in
 int orc_iteration(void* p, int stage, int iter_index, int n_threads) {
   Oracle* o = static_cast<Oracle*>(p);
   return guarded(o, [&]() {
-    rng.randomEngine.seed_with(o->seed);
+    rng_reseed(o->seed);
     phase_iteration(*o, stage, iter_index, n_threads);
   });
 }
@@ -418,8 +444,8 @@ int orc_pbwt_select(void* p, int iter_index, int main_iteration) {
   return guarded(o, [&]() {
     o->H.updateHaplotypes(o->G);
     o->H.transposeRareTar();
-    rng.randomEngine.seed_with(o->seed);
-    rng.randomEngine.select(gp::RNG_PBWT, iter_index, 0);
+    rng_reseed(o->seed);
+    rng_select(gp::RNG_PBWT, iter_index, 0);
     o->H.matchHapsFromCompressedPBWTSmall(o->V, main_iteration != 0);
   });
 }
@@ -542,8 +568,8 @@ int orc_rephase(void* p, const uint32_t* states, int K, uint8_t* H0, uint8_t* H1
       h1[l] = H1[l] != 0;
       fl[l] = flat[l] != 0;
     }
-    rng.randomEngine.seed_with(o->seed);
-    rng.randomEngine.select(gp::RNG_PHASE, iter_index, target);
+    rng_reseed(o->seed);
+    rng_select(gp::RNG_PHASE, iter_index, target);
     D.rephaseHaplotypes(h0, h1, fl);
     for (int l = 0; l < L; ++l) {
       H0[l] = h0[l];
@@ -572,7 +598,8 @@ void orc_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
   gp::philox4x32_10(ctr[0], ctr[1], ctr[2], ctr[3], key[0], key[1], out);
 }
 
-// getFloat / getInt through the shimmed reference RNG class.
+#ifndef GP_NATIVE_RNG
+// getFloat / getInt through the shimmed reference RNG class (replay build only).
 void orc_rng_floats(uint64_t seed, uint32_t purpose, uint32_t iteration, uint32_t target, int n, float* out) {
   random_number_generator r;
   r.randomEngine.seed_with(seed);
@@ -601,5 +628,9 @@ int orc_std_sample(uint64_t seed, uint32_t purpose, uint32_t iteration, uint32_t
   *words_used = r.randomEngine.pos;
   return (int)s.size();
 }
+#endif  // GP_NATIVE_RNG
+
+// 1 in the native-RNG build (the reference's own std::mt19937), 0 in the replay build.
+int orc_native_rng() { return kNativeRng ? 1 : 0; }
 
 }  // extern "C"

@@ -7,8 +7,16 @@
  * yields the words of one counter-based stream (glimpse_b200/csrc/replay_rng.h).
  * The oracle driver selects the stream (purpose, iteration, target) before each
  * reference call, so the reference code and the GPU kernels consume the same
- * words. `rng` is thread_local so that threaded oracle runs stay reproducible. */
+ * words. `rng` is thread_local so that threaded oracle runs stay reproducible.
+ *
+ * With GP_NATIVE_RNG defined (the native-RNG oracle build) this header instead
+ * includes the reference's own random_number.h, unmodified: std::mt19937 seeded
+ * once, drawn in the reference's call order on one thread. */
 #pragma once
+#ifdef GP_NATIVE_RNG
+#include <cmath>
+#include_next <utils/random_number.h>
+#else
 #include <cfloat>
 #include <cstdint>
 #include <random>
@@ -86,3 +94,4 @@ public:
     return vec.size() - 1;
   }
 };
+#endif  // GP_NATIVE_RNG

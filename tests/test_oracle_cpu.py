@@ -157,6 +157,39 @@ def test_reference_driver_runs(small_workload):
     assert synth.dosage_r2(np.stack(ds), w.targets.truth.sum(1)) > 0.5
 
 
+def test_reference_with_its_own_generator():
+    """The native-RNG oracle build runs the reference with its own std::mt19937
+    (random_number.h:35-125, seeded once as caller_initialise.cpp:49). The run is
+    reproducible for a seed, draws differently from the replay streams, reaches
+    the same dosage r2 within sampling noise, and refuses more than one thread
+    (the reference's generator is one global stream)."""
+    from oracle import oracle as O
+    if not O.ref_available(native_rng=True):
+        pytest.skip("oracle/_ref native build missing")
+    from glimpse_b200 import synth
+    w = synth.make_panel_and_targets(800, 6000, 1.0, 0.5, 4, ("uniform", 0.5, 2.0), ("fixed", 150), seed=7,
+                                     sparse_maf=0.005)
+    kw = dict(kinit=300, kpbwt=150, pbwt_depth=8, pbwt_modulo_cm=0.05)
+    truth = w.targets.truth.sum(1)
+
+    def run(native):
+        orc = O.RefOracle(w.panel, w.targets, native_rng=native, **kw)
+        orc.run(burnin=5, main=15)
+        ds = []
+        for t in range(w.targets.n):
+            g0, g1, _, _, _ = orc.gp(t)
+            ds.append(g1 + 2 * np.clip(1 - g0 - g1, 0, 1))
+        return np.stack(ds)
+
+    a, b, replay = run(True), run(True), run(False)
+    assert np.array_equal(a, b)
+    assert not np.array_equal(a, replay)
+    assert abs(synth.dosage_r2(a, truth) - synth.dosage_r2(replay, truth)) <= 0.01
+    orc = O.RefOracle(w.panel, w.targets, native_rng=True, **kw)
+    with pytest.raises(RuntimeError, match="one thread"):
+        orc.iteration(O.STAGE_INIT, 0, threads=2)
+
+
 def test_reference_state_lists(small_workload):
     """The reference's --state-list path as the oracle runs it
     (conditioning_set.cpp:114-121): every set holds the union of its target's
