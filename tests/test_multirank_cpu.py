@@ -69,3 +69,34 @@ def test_single_rank_ops_are_identity():
     barrier, mx = bench.rank_ops(None, None)
     barrier()
     assert mx(3.5) == 3.5
+
+
+@pytest.mark.parametrize("rng", ["replay", "native"])
+def test_reference_arm_line(rng, monkeypatch):
+    """Rank 0 of the reference arm prints one JSON line with the contract's keys:
+    the reference's host run of the small workload (one complete run), its
+    cpu_baseline (kind "reference", the threads used: one with the reference's
+    own generator) and an e2e block with no host-device copies."""
+    import json
+    sys.path.insert(0, ROOT)
+    import bench
+    from oracle import oracle as O
+    if not O.ref_available(native_rng=rng == "native"):
+        pytest.skip("oracle/_ref not built")
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
+        monkeypatch.delenv(k, raising=False)
+    args = type("A", (), dict(gpus=1, steps=1, warmup=0, config="small", impl="reference", subset=0,
+                              ref_rng=rng))()
+    buf = io.StringIO()
+    with redirect_stdout(buf):
+        assert bench.run_reference(args) == 0
+    line = json.loads(buf.getvalue().strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["unit"] == "samples/s" and line["value"] > 0
+    assert line["config"]["rng"] == rng and line["config"]["targets_timed"] == 1
+    cb = line["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["value"] == line["value"]
+    if rng == "native":
+        assert cb["cores"] == 1
+    assert line["e2e"] == {"value": line["value"], "unit": "samples/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
+    assert 0.5 < line["dosage_r2"] <= 1.0
